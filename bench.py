@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark of the batched complex FFT path on B200.
+
+Workload (one step): C2C FFT of N=4096 x 16384 complex64 lines, re and im
+i.i.d. N(0,1) from a fixed seed, interleaved layout, forward, FP32 storage --
+the tensor-core comparison workload (512 MiB read + 512 MiB written per step,
+larger than the 126 MB L2, so no flush is needed between steps).  The
+FP32 Stockham kernel and the tcgen05 split-FP16 kernel are both timed; the
+headline `value` is the faster of those whose relative RMS error against an
+FP64 FFT of sampled lines is <= 3e-6.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank transforms its own 16384 lines (weak scaling, no
+collective on the data path); rank 0 prints one JSON line.
+`--impl reference` times the reference's algorithm on the host cores instead
+(the FP32 radix-4 Stockham restatement in oracle/, OpenMP over lines; the
+reference's own CPU path is Apple vDSP, which does not exist on Linux).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 4096
+BATCH = 16384
+SEED = 20261203
+ERR_BAR = 3e-6
+METRIC = "FP32 vs split-FP16 tensor-core FFT: transforms/s, % HBM peak at <=3e-6 rel err"
+BYTES_PER_TRANSFORM = N * 8 * 2  # read + write, complex64
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--batch", type=int, default=BATCH)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_launch(kernel):
+    """DRAM bytes per launch from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    v = d.get(kernel)
+    return v.get("bytes_per_launch") if isinstance(v, dict) else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [s.strip() for s in line.split(",")]
+                if len(parts) < 10:
+                    continue
+                if self.uuid and self.uuid not in parts[1]:
+                    continue
+                rows.append(parts)
+        except OSError:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def make_input(batch, rank):
+    import numpy as np
+    rng = np.random.default_rng(SEED + rank)
+    z = rng.standard_normal(size=(batch, N, 2), dtype=np.float32)
+    return z.view(np.complex64)[..., 0]
+
+
+def fp64_check(x_rows, y_rows):
+    """rel RMS of y against an FP64 FFT (numpy pocketfft) of x."""
+    import numpy as np
+    ref = np.fft.fft(x_rows.astype(np.complex128), axis=-1)
+    return float(np.linalg.norm(y_rows - ref) / np.linalg.norm(ref))
+
+
+def cpu_baseline(seconds=12.0):
+    """The reference algorithm (FP32 radix-4 Stockham, oracle/) on all host
+    cores over a bounded sample of the same workload."""
+    from oracle import oracle as O
+    sample = 1024
+    x = O.normal_c64((sample, N), seed=SEED)
+    O.ref_fft(x[:64])  # warm
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        O.ref_fft(x)
+        reps += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": reps * sample / dt, "unit": "transforms/s", "cores": O.max_threads(),
+            "kind": "port",
+            "sample": "%d x %d lines of N=%d (of the 16384-line step), FP32 radix-4 Stockham "
+                      "restatement of the reference, OpenMP over lines" % (reps, sample, N)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    sample = 512
+    x = O.normal_c64((sample, N), seed=SEED)
+    for _ in range(args.warmup):
+        O.ref_fft(x)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.ref_fft(x)
+    dt = time.perf_counter() - t0
+    v = args.steps * sample / dt
+    cores = O.max_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "transforms/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "batched C2C FFT N=4096, complex64 N(0,1) seeded; each step a "
+                               "bounded sample of %d of the 16384 lines" % sample,
+                   "n": N, "batch": sample},
+        "cpu_baseline": {"value": v, "unit": "transforms/s", "cores": cores, "kind": "port",
+                         "sample": "%d lines of N=%d per step, FP32 radix-4 Stockham restatement "
+                                   "of the reference, OpenMP over lines" % (sample, N)},
+        "e2e": {"value": v, "unit": "transforms/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import ctypes
+    from datetime import timedelta
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    import metalfft_b200 as M
+
+    B = args.batch
+    host = make_input(B, rank)
+    x = torch.from_numpy(host).cuda()
+    y = torch.empty_like(x)
+    f = M.MetalFFT(N)
+    stream = torch.cuda.current_stream()
+
+    variants = {"fp32": 0, "tc_fp16_split3": M.TC_FP16_SPLIT3, "tc_bf16": M.TC_BF16}
+
+    rows = np.random.default_rng(1).choice(B, 16, replace=False)
+    results = {}
+    peak, peak_src = peaks()
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+
+    for name, tc in list(variants.items()):
+        try:
+            f.exec(x, y, B, M.FORWARD, tc)
+        except M.FFTError as e:
+            if name == "fp32":
+                raise
+            results[name] = {"unavailable": str(e)}
+            continue
+        torch.cuda.synchronize()
+        err = fp64_check(host[rows], y[torch.from_numpy(rows).cuda()].cpu().numpy())
+        for _ in range(max(3, args.warmup)):
+            f.exec(x, y, B, M.FORWARD, tc)
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(uuid) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                f.exec(x, y, B, M.FORWARD, tc)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        t = torch.tensor([ms], device="cuda")
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        per_launch_s = ms / args.steps / 1e3
+        gbs = BYTES_PER_TRANSFORM * B / per_launch_s / 1e9
+        results[name] = {
+            "transforms_per_s": B * world * args.steps / (ms_max / 1e3),
+            "ms_per_step": ms_max / args.steps,
+            "rel_rms": err,
+            "hbm_gbs": gbs,
+            "frac": gbs / peak,
+            "clocks": clk.summary(),
+        }
+
+    ok = {k: v for k, v in results.items() if "rel_rms" in v and v["rel_rms"] <= ERR_BAR}
+    best = max(ok, key=lambda k: ok[k]["transforms_per_s"]) if ok else "fp32"
+    r = results[best]
+
+    # e2e through the public C ABI with host buffers (pinned), copies included
+    hin = torch.from_numpy(host).pin_memory()
+    hout = torch.empty_like(hin).pin_memory()
+    tc = variants[best]
+
+    def e2e_call():
+        if tc:
+            st = M.lib.mfft_exec_c2c_tc(f._plan, ctypes.c_void_p(hin.data_ptr()),
+                                        ctypes.c_void_p(hout.data_ptr()), B, M.FORWARD, tc,
+                                        M.HOST, None)
+        else:
+            st = M.lib.mfft_exec_c2c(f._plan, ctypes.c_void_p(hin.data_ptr()),
+                                     ctypes.c_void_p(hout.data_ptr()), B, M.FORWARD, M.HOST, None)
+        M._check(st)
+
+    e2e_call()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_call()
+    barrier()
+    dt = time.perf_counter() - t0
+    tt = torch.tensor([dt], device="cuda")
+    if dist is not None:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e = {"value": B * world * args.e2e_steps / float(tt.item()), "unit": "transforms/s",
+           "h2d_bytes_per_step": B * N * 8, "d2h_bytes_per_step": B * N * 8,
+           "steps": args.e2e_steps}
+
+    kernel_name = "k_fft_batched" if best == "fp32" else "k_fft4096_tc"
+    line = {
+        "metric": METRIC,
+        "value": r["transforms_per_s"],
+        "unit": "transforms/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": r["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32" if best == "fp32" else ("fp16x3->fp32" if best == "tc_fp16_split3" else "bf16->fp32"),
+        "data": "synthetic",
+        "config": {"workload": "batched C2C FFT N=4096 x 16384 lines per GPU, complex64, re/im "
+                               "N(0,1) seeded, forward",
+                   "n": N, "batch_per_gpu": B, "variant": best, "parallelism": "replicas",
+                   "l2": "inputs larger than L2 (512 MiB read + 512 MiB written per step)"},
+        "rel_rms": r["rel_rms"],
+        "variants": results,
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": r["hbm_gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": r["hbm_gbs"] / peak, "peak_source": peak_src,
+                     "traffic": traffic_per_launch(kernel_name),
+                     "algorithmic_bytes_per_launch": BYTES_PER_TRANSFORM * B},
+        "clocks": r["clocks"],
+        "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

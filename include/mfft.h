@@ -1,0 +1,237 @@
+/*
+ * mfft.h -- C ABI of libmfft.so, the B200 (sm_100a) implementation of
+ * MetalFFT's batched complex FFT path and its direct callers.
+ *
+ * The reference's public boundary is a Swift API (docs/MetalFFT.swiftinterface
+ * :12-266).  Every entry point below names the Swift declaration it replaces;
+ * a Swift/C++/Python wrapper re-creates that API on top (the Swift module map
+ * and wrapper are given in INTEGRATION.md, the Python mirror is
+ * metalfft_b200/__init__.py, the C++ mirror is metalfft_b200/MetalFFT.hpp).
+ *
+ * Conventions
+ *  - Complex data is interleaved complex64: {float re, float im} per element
+ *    (the reference's SIMD2<Float>), transform b of a batch at offset b*n.
+ *  - Forward is unscaled with the e^{-2*pi*i*j*k/n} kernel
+ *    (Sources/MetalFFT/Resources/fft_multisize.metal:70); inverse is
+ *    (1/n) * conj(FFT(conj(X))) (Sources/MetalFFT/FFT/MetalFFT.swift:56-65).
+ *  - Every function returns an mfft_status; nothing aborts and nothing traps
+ *    on the device.  The text of the last error on the calling thread is
+ *    returned by mfft_last_error().
+ *  - flags: MFFT_HOST_MEMORY (default) means the pointers are host memory;
+ *    the call copies in, runs and copies out before returning, which is the
+ *    Swift arrays' semantics (MetalFFT.swift:74-84, synchronous like
+ *    commitAndWait, Internal/Dispatch.swift:3-10).  MFFT_DEVICE_MEMORY means
+ *    the pointers are device memory and the work is only enqueued on
+ *    `stream` (a cudaStream_t; NULL = the legacy default stream).
+ *  - Handles are single-writer: one thread at a time per handle
+ *    (MetalFFT.swift:9).  Context creation is thread-safe.
+ */
+#ifndef MFFT_H
+#define MFFT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MFFT_API __attribute__((visibility("default")))
+#else
+#define MFFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1..9 map one-to-one onto the cases of FFTError
+ * (Sources/MetalFFT/Internal/MetalContext.swift:6-30). */
+typedef enum mfft_status {
+    MFFT_SUCCESS = 0,
+    MFFT_ERR_NO_DEVICE = 1,          /* FFTError.noMetalDevice            */
+    MFFT_ERR_NO_STREAM = 2,          /* FFTError.noCommandQueue           */
+    MFFT_ERR_LIBRARY_BUILD = 3,      /* FFTError.libraryBuildFailed       */
+    MFFT_ERR_KERNEL_NOT_FOUND = 4,   /* FFTError.kernelNotFound           */
+    MFFT_ERR_EXEC_FAILED = 5,        /* FFTError.commandBufferFailed      */
+    MFFT_ERR_INVALID_INPUT_SIZE = 6, /* FFTError.invalidInputSize         */
+    MFFT_ERR_BATCH_INPUT_SIZE = 7,   /* FFTError.batchInputSize           */
+    MFFT_ERR_UNSUPPORTED_SIZE = 8,   /* FFTError.unsupportedFFTSize       */
+    MFFT_ERR_ALLOCATION = 9,         /* FFTError.bufferAllocationFailed   */
+    MFFT_ERR_INVALID_ARGUMENT = 10,  /* Swift precondition() traps        */
+    MFFT_ERR_TIMEOUT = 11            /* a bounded device-side wait expired */
+} mfft_status;
+
+enum {
+    MFFT_HOST_MEMORY = 0,
+    MFFT_DEVICE_MEMORY = 1
+};
+
+enum {
+    MFFT_FORWARD = -1,
+    MFFT_INVERSE = +1
+};
+
+/* Tensor-core variants for mfft_exec_c2c_tc. */
+enum {
+    MFFT_TC_FP16_SPLIT3 = 1, /* hi/lo FP16 split, 3 products, FP32 accumulate */
+    MFFT_TC_BF16 = 2         /* plain BF16 operands, FP32 accumulate          */
+};
+
+/* Window kinds (Sources/MetalFFT/DSP/Window.swift:6-24, WindowType). */
+enum {
+    MFFT_WINDOW_HANN = 0,
+    MFFT_WINDOW_HAMMING = 1,
+    MFFT_WINDOW_BLACKMAN = 2,
+    MFFT_WINDOW_FLAT_TOP = 3,
+    MFFT_WINDOW_KAISER = 4,
+    MFFT_WINDOW_RECTANGULAR = 5
+};
+
+typedef struct mfft_ctx mfft_ctx;
+typedef struct mfft_plan mfft_plan;
+typedef struct mfft_conv mfft_conv;
+typedef struct mfft_corr mfft_corr;
+typedef struct mfft_analyzer mfft_analyzer;
+typedef struct mfft_multi mfft_multi;
+
+/* ---- errors ------------------------------------------------------------ */
+
+/* Static text for a status code (FFTError.description, MetalContext.swift:19-29). */
+MFFT_API const char* mfft_status_string(int status);
+
+/* Copies the calling thread's last error text (with expected/got/index where
+ * the FFTError case carries them) into buf; returns that status. */
+MFFT_API int mfft_last_error(char* buf, size_t len);
+
+/* The integer payload of the calling thread's last error:
+ * invalidInputSize(expected, got) / batchInputSize(expected, got, batchIndex) /
+ * unsupportedFFTSize(n) -> expected = n.  Unused fields are -1. */
+MFFT_API int mfft_last_error_detail(int64_t* expected, int64_t* got, int64_t* index);
+
+/* ---- context (MetalContext.shared(), MetalContext.swift:74-142) --------- */
+
+/* The process-wide context for the current CUDA device: created on first use
+ * under a lock, then shared.  Never destroy the shared context. */
+MFFT_API int mfft_context_shared(mfft_ctx** out);
+/* A private context on `device` (-1 = current device). */
+MFFT_API int mfft_context_create(int device, mfft_ctx** out);
+MFFT_API int mfft_context_destroy(mfft_ctx* ctx);
+/* Number of SMs of the context's device (grid sizing). */
+MFFT_API int mfft_context_sm_count(const mfft_ctx* ctx);
+
+/* ---- plans: MetalFFT.init(size:) (MetalFFT.swift:27-51) ---------------- */
+
+/* n: power of two in [64, 2^20].  The reference accepts 64..16384
+ * (FFTDescriptor, MetalContext.swift:47-69) and throws unsupportedFFTSize
+ * otherwise; sizes above 16384 use the four-step path. */
+MFFT_API int mfft_plan_create(mfft_ctx* ctx, int64_t n, mfft_plan** out);
+MFFT_API int mfft_plan_destroy(mfft_plan* plan);
+MFFT_API int64_t mfft_plan_size(const mfft_plan* plan);
+/* Smallest supported size for a kernel of kernel_count taps in the reference's
+ * size list, or 0 (Convolver.recommendedFFTSize, Convolve.swift:83-86). */
+MFFT_API int64_t mfft_recommended_fft_size(int64_t kernel_count);
+
+/* Autotuner (no reference counterpart; the reference hard-codes one kernel
+ * per size, MetalContext.swift:47-69): times every registered radix /
+ * lines-per-CTA variant of the batched kernel for size n (64..16384) over
+ * `lines` lines (<= 0: 256 MiB worth) and keeps the fastest for this context;
+ * appends "n radix lines_per_cta" to the file named by $MFFT_TUNE_CACHE, which
+ * later plans read.  Reports the choice. */
+MFFT_API int mfft_autotune(mfft_ctx* ctx, int64_t n, int64_t lines, int* radix, int* lines_per_cta);
+/* Pins a plan (n <= 16384) to one registered variant: main radix 8 or 16 and
+ * lines per CTA.  MFFT_ERR_KERNEL_NOT_FOUND if that variant is not built. */
+MFFT_API int mfft_plan_set_kernel(mfft_plan* plan, int radix, int lines_per_cta);
+/* Lists the registered variants for size n: fills up to cap (radix,
+ * lines_per_cta) pairs and returns how many exist (host only). */
+MFFT_API int mfft_list_kernels(int64_t n, int* radix, int* lines_per_cta, int cap);
+/* The kernel a plan uses: main radix, lines per CTA, threads per CTA. */
+MFFT_API int mfft_plan_kernel_info(const mfft_plan* plan, int* radix, int* lines_per_cta, int* threads);
+
+/* ---- execution --------------------------------------------------------- */
+
+/* Batched C2C.  Replaces forward(_:) (batch = 1, MetalFFT.swift:69-85),
+ * forward(input:output:) (MetalFFT.swift:88-104), forward(batch:)
+ * (MetalFFT.swift:108-133), inverse(_:) (MetalFFT.swift:56-65) and
+ * MultiChannelFFT.forward/inverse (MultiChannelFFT.swift:37-53).
+ * direction: MFFT_FORWARD or MFFT_INVERSE (1/n scaled).  batch >= 0
+ * (batch == 0 returns at once, as forward(batch: []) returns []).  in == out
+ * is allowed. */
+MFFT_API int mfft_exec_c2c(mfft_plan* plan, const void* in, void* out, int64_t batch, int direction,
+                  int flags, void* stream);
+
+/* Tensor-core DFT-as-matmul path (tcgen05 + TMEM) for n = 4096: the B200 form
+ * of src/fft_4096_ct_mma.metal:88-206 (simdgroup_float8x8 CT-DIF).  variant:
+ * MFFT_TC_FP16_SPLIT3 or MFFT_TC_BF16.  Same layout and scaling as
+ * mfft_exec_c2c. */
+MFFT_API int mfft_exec_c2c_tc(mfft_plan* plan, const void* in, void* out, int64_t batch,
+                     int direction, int variant, int flags, void* stream);
+
+/* ---- mixed sizes in one persistent launch ------------------------------ */
+
+/* One size class: `count` transforms of length n (power of two, 64..2^20)
+ * stored back to back starting at complex element `offset` of the in/out
+ * buffers.  There is no reference counterpart for a single launch over mixed
+ * sizes; it generalises forward(batch:) (MetalFFT.swift:108-133). */
+typedef struct mfft_multi_desc {
+    int64_t n;
+    int64_t count;
+    int64_t offset;
+} mfft_multi_desc;
+
+MFFT_API int mfft_multi_create(mfft_ctx* ctx, const mfft_multi_desc* descs, int ndesc,
+                      mfft_multi** out);
+MFFT_API int mfft_multi_destroy(mfft_multi* m);
+/* Total complex elements covered by the descriptors (in and out size). */
+MFFT_API int64_t mfft_multi_points(const mfft_multi* m);
+MFFT_API int mfft_multi_exec(mfft_multi* m, const void* in, void* out, int direction, int flags,
+                    void* stream);
+
+/* ---- Convolver (Convolve.swift:8-87) / FusedConvolver ------------------- */
+
+/* kernel_len < fft_size (the precondition of Convolve.swift:20-21).  The
+ * kernel spectrum is computed once on the device (Convolve.swift:27-31). */
+MFFT_API int mfft_conv_create(mfft_ctx* ctx, const float* kernel, int64_t kernel_len, int64_t fft_size,
+                     mfft_conv** out);
+MFFT_API int mfft_conv_destroy(mfft_conv* conv);
+MFFT_API int64_t mfft_conv_block_size(const mfft_conv* conv); /* Convolver.blockSize */
+MFFT_API int64_t mfft_conv_hop_size(const mfft_conv* conv);   /* Convolver.hopSize   */
+MFFT_API int64_t mfft_conv_kernel_len(const mfft_conv* conv);
+/* Convolver.apply(to:) / FusedConvolver.apply(to:): out has n + kernel_len - 1
+ * samples (Convolve.swift:36-76).  n == 0 gives kernel_len - 1 zeros. */
+MFFT_API int mfft_conv_apply(mfft_conv* conv, const float* signal, int64_t n, float* out, int flags,
+                    void* stream);
+/* Adjoint of apply for a loss L with grad_out = dL/dout (n + kernel_len - 1
+ * samples): grad_signal (n samples) and grad_kernel (kernel_len samples).
+ * Either output may be NULL.  No reference counterpart (the reference has no
+ * backward pass). */
+MFFT_API int mfft_conv_backward(mfft_conv* conv, const float* signal, int64_t n, const float* grad_out,
+                       float* grad_signal, float* grad_kernel, int flags, void* stream);
+
+/* ---- Correlator (Correlate.swift:7-62) --------------------------------- */
+
+MFFT_API int mfft_corr_create(mfft_ctx* ctx, int64_t fft_size, mfft_corr** out);
+MFFT_API int mfft_corr_destroy(mfft_corr* corr);
+/* cross(_:_:): out = Re IFFT(FFT(a) * conj(FFT(b))) over fft_size, i.e.
+ * out[m] = sum_n a[(n+m) mod fft_size] b[n], inputs zero-padded or truncated
+ * to fft_size (Correlate.swift:31-61; the code's lag convention -- its doc
+ * comment writes the mirrored sum_n a[n] b[n+m]); fft_size samples written.
+ * auto(_:) is cross(a, a). */
+MFFT_API int mfft_corr_cross(mfft_corr* corr, const float* a, int64_t na, const float* b, int64_t nb,
+                    float* out, int flags, void* stream);
+
+/* ---- FFTAnalyzer (FFTAnalyzer.swift:68-117) ----------------------------- */
+
+/* window coefficients of WindowType.coefficients (Window.swift:12-23). */
+MFFT_API int mfft_window(int kind, int64_t n, double kaiser_beta, float* out);
+MFFT_API int mfft_analyzer_create(mfft_ctx* ctx, int64_t size, double sample_rate, int window_kind,
+                         double kaiser_beta, mfft_analyzer** out);
+MFFT_API int mfft_analyzer_destroy(mfft_analyzer* a);
+/* analyze(_:offset:): window samples[offset .. offset+size) and FFT them;
+ * spectrum receives `size` complex64 bins.  Requires offset + size <= count
+ * (the precondition of FFTAnalyzer.swift:108). */
+MFFT_API int mfft_analyzer_analyze(mfft_analyzer* a, const float* samples, int64_t count,
+                          int64_t offset, void* spectrum, int flags, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MFFT_H */

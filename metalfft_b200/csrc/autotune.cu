@@ -1,0 +1,165 @@
+// autotune.cu -- per-size choice of the batched kernel (radix E, lines per
+// CTA) by timing the candidates on the device, cached per context and on disk.
+//
+// The reference fixes one kernel and thread count per size in a switch
+// (FFTDescriptor, Sources/MetalFFT/Internal/MetalContext.swift:47-69; N=4096
+// batches switch to the radix-8 kernel, MetalFFT.swift:163-165).  Here every
+// registered instantiation for the size is timed with CUDA events on a batch
+// larger than L2 and the fastest is kept.  The cache file (one line
+// "n e fpb" per size) is read from $MFFT_TUNE_CACHE when that is set.
+#include <stdio.h>
+#include <stdlib.h>
+
+#include <vector>
+
+#include "capi_internal.h"
+
+namespace mfft {
+
+static bool read_cache(int n, int* e, int* fpb) {
+    const char* path = getenv("MFFT_TUNE_CACHE");
+    if (!path || !*path) return false;
+    FILE* f = fopen(path, "r");
+    if (!f) return false;
+    int cn, ce, cf;
+    bool found = false;
+    while (fscanf(f, "%d %d %d", &cn, &ce, &cf) == 3) {
+        if (cn == n) {
+            *e = ce;
+            *fpb = cf;
+            found = true;
+        }
+    }
+    fclose(f);
+    return found;
+}
+
+static void write_cache(int n, int e, int fpb) {
+    const char* path = getenv("MFFT_TUNE_CACHE");
+    if (!path || !*path) return;
+    FILE* f = fopen(path, "a");
+    if (!f) return;
+    fprintf(f, "%d %d %d\n", n, e, fpb);
+    fclose(f);
+}
+
+const BatchedKernel* tuned_batched(mfft_ctx* ctx, int n) {
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        auto it = ctx->tuned.find(n);
+        if (it != ctx->tuned.end()) return it->second;
+    }
+    const BatchedKernel* k = nullptr;
+    int e = 0, fpb = 0;
+    if (read_cache(n, &e, &fpb)) k = find_batched(n, e, fpb);
+    if (!k) k = default_batched(n);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->tuned[n] = k;
+    return k;
+}
+
+// Times every registered candidate for size n on `lines` lines and installs
+// the fastest in the context.  Returns the chosen kernel through out.
+int autotune_batched(mfft_ctx* ctx, int n, long long lines, const BatchedKernel** out) {
+    DeviceGuard g(ctx->device);
+    int cnt = 0;
+    const BatchedKernel* ks = batched_kernels(&cnt);
+    size_t bytes = (size_t)lines * n * sizeof(float2);
+    float2 *a = nullptr, *b = nullptr;
+    if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess) {
+        cudaFree(a);
+        return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "autotune buffers");
+    }
+    cudaMemsetAsync(a, 0, bytes, ctx->stream);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const BatchedKernel* best = nullptr;
+    float best_ms = 1e30f;
+    for (int i = 0; i < cnt; ++i) {
+        if (ks[i].n != n) continue;
+        BatchedBinding bb;
+        if (bind_batched(ctx, &ks[i], &bb) != MFFT_SUCCESS) continue;
+        for (int w = 0; w < 3; ++w) ks[i].fwd(a, b, lines, bb.tw, ctx->stream);
+        cudaEventRecord(e0, ctx->stream);
+        const int reps = 10;
+        for (int r = 0; r < reps; ++r) ks[i].fwd((r & 1) ? b : a, (r & 1) ? a : b, lines, bb.tw, ctx->stream);
+        cudaEventRecord(e1, ctx->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) continue;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = &ks[i];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(a);
+    cudaFree(b);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return cuda_error(err, "autotune");
+    if (!best) return set_error(MFFT_ERR_KERNEL_NOT_FOUND, -1, -1, -1, "no kernel for n=%d", n);
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ctx->tuned[n] = best;
+    }
+    write_cache(n, best->e, best->fpb);
+    *out = best;
+    return MFFT_SUCCESS;
+}
+
+}  // namespace mfft
+
+extern "C" int mfft_autotune(mfft_ctx* ctx, int64_t n, int64_t lines, int* radix, int* lines_per_cta) {
+    using namespace mfft;
+    if (!ctx) {
+        int st = mfft_context_shared(&ctx);
+        if (st) return st;
+    }
+    if (!is_pow2_in(n, 64, MFFT_MAX_SINGLE_N))
+        return set_error(MFFT_ERR_UNSUPPORTED_SIZE, n, -1, -1, "autotune covers 64..16384, got %lld", (long long)n);
+    if (lines <= 0) lines = (int64_t)(256ll << 20) / (n * 8);  // 256 MiB, twice L2
+    const BatchedKernel* k = nullptr;
+    int st = autotune_batched(ctx, (int)n, lines, &k);
+    if (st) return st;
+    if (radix) *radix = k->e;
+    if (lines_per_cta) *lines_per_cta = k->fpb;
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_plan_kernel_info(const mfft_plan* plan, int* radix, int* lines_per_cta, int* threads) {
+    if (!plan) return mfft::set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "plan is NULL");
+    const mfft::BatchedKernel* k = plan->line.k;
+    if (radix) *radix = k ? k->e : 16;
+    if (lines_per_cta) *lines_per_cta = k ? k->fpb : 0;
+    if (threads) *threads = k ? k->threads : 0;
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_plan_set_kernel(mfft_plan* plan, int radix, int lines_per_cta) {
+    using namespace mfft;
+    if (!plan) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "plan is NULL");
+    if (plan->n > MFFT_MAX_SINGLE_N)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "n=%lld uses the four-step path", (long long)plan->n);
+    const BatchedKernel* k = find_batched((int)plan->n, radix, lines_per_cta);
+    if (!k)
+        return set_error(MFFT_ERR_KERNEL_NOT_FOUND, -1, -1, -1, "no variant n=%lld radix=%d lines_per_cta=%d",
+                         (long long)plan->n, radix, lines_per_cta);
+    DeviceGuard g(plan->ctx->device);
+    return bind_batched(plan->ctx, k, &plan->line);
+}
+
+extern "C" int mfft_list_kernels(int64_t n, int* radix, int* lines_per_cta, int cap) {
+    int cnt = 0, m = 0;
+    const mfft::BatchedKernel* ks = mfft::batched_kernels(&cnt);
+    for (int i = 0; i < cnt; ++i) {
+        if (ks[i].n != n) continue;
+        if (m < cap) {
+            if (radix) radix[m] = ks[i].e;
+            if (lines_per_cta) lines_per_cta[m] = ks[i].fpb;
+        }
+        ++m;
+    }
+    return m;
+}

@@ -1,0 +1,356 @@
+// capi.cu -- the extern "C" boundary of libmfft (include/mfft.h): contexts,
+// plans, error reporting and the batched C2C entry points.
+//
+// Mirrors the reference runtime (Sources/MetalFFT/Internal/MetalContext.swift,
+// Dispatch.swift, Sources/MetalFFT/FFT/MetalFFT.swift): a lock-protected
+// process-wide context per device (MetalContext.shared, :74-88), a plan per
+// size (FFTDescriptor, :34-70), synchronous host-array calls that surface a
+// failed execution as MFFT_ERR_EXEC_FAILED (commitAndWait, Dispatch.swift:3-10).
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+
+#include "capi_internal.h"
+
+using namespace mfft;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+
+namespace {
+struct ErrState {
+    int status = MFFT_SUCCESS;
+    std::string msg;
+    int64_t expected = -1, got = -1, index = -1;
+};
+thread_local ErrState g_err;
+}  // namespace
+
+namespace mfft {
+
+int set_error(int status, int64_t expected, int64_t got, int64_t index, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err.status = status;
+    g_err.msg = buf;
+    g_err.expected = expected;
+    g_err.got = got;
+    g_err.index = index;
+    return status;
+}
+
+int cuda_error(cudaError_t e, const char* what) {
+    return set_error(e == cudaErrorMemoryAllocation ? MFFT_ERR_ALLOCATION : MFFT_ERR_EXEC_FAILED, -1,
+                     -1, -1, "Command buffer error: %s: %s", what, cudaGetErrorString(e));
+}
+
+DeviceGuard::DeviceGuard(int dev) {
+    cudaGetDevice(&prev_);
+    if (prev_ != dev) cudaSetDevice(dev);
+}
+DeviceGuard::~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != prev_) cudaSetDevice(prev_);
+}
+
+bool is_pow2_in(int64_t n, int64_t lo, int64_t hi) {
+    return n >= lo && n <= hi && (n & (n - 1)) == 0;
+}
+
+}  // namespace mfft
+
+extern "C" const char* mfft_status_string(int status) {
+    switch (status) {
+        case MFFT_SUCCESS: return "success";
+        case MFFT_ERR_NO_DEVICE: return "No CUDA device available";
+        case MFFT_ERR_NO_STREAM: return "Could not create CUDA stream";
+        case MFFT_ERR_LIBRARY_BUILD: return "Kernel image not loadable on this device (needs sm_100a)";
+        case MFFT_ERR_KERNEL_NOT_FOUND: return "Kernel not found";
+        case MFFT_ERR_EXEC_FAILED: return "Command buffer error";
+        case MFFT_ERR_INVALID_INPUT_SIZE: return "Input size mismatch";
+        case MFFT_ERR_BATCH_INPUT_SIZE: return "Batch element size mismatch";
+        case MFFT_ERR_UNSUPPORTED_SIZE: return "Unsupported FFT size";
+        case MFFT_ERR_ALLOCATION: return "Device buffer allocation failed";
+        case MFFT_ERR_INVALID_ARGUMENT: return "Invalid argument";
+        case MFFT_ERR_TIMEOUT: return "Device-side wait timed out";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int mfft_last_error(char* buf, size_t len) {
+    if (buf && len) {
+        size_t n = g_err.msg.size() < len - 1 ? g_err.msg.size() : len - 1;
+        memcpy(buf, g_err.msg.data(), n);
+        buf[n] = 0;
+    }
+    return g_err.status;
+}
+
+extern "C" int mfft_last_error_detail(int64_t* expected, int64_t* got, int64_t* index) {
+    if (expected) *expected = g_err.expected;
+    if (got) *got = g_err.got;
+    if (index) *index = g_err.index;
+    return g_err.status;
+}
+
+// ---------------------------------------------------------------------------
+// contexts
+// ---------------------------------------------------------------------------
+
+static int ctx_init(int device, mfft_ctx** out) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return set_error(MFFT_ERR_NO_DEVICE, -1, -1, -1, "No CUDA device available (%s)",
+                         cudaGetErrorString(e));
+    if (device < 0) {
+        if (cudaGetDevice(&device) != cudaSuccess) device = 0;
+    }
+    if (device >= count)
+        return set_error(MFFT_ERR_NO_DEVICE, -1, -1, -1, "CUDA device %d does not exist (%d present)",
+                         device, count);
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return set_error(MFFT_ERR_NO_DEVICE, -1, -1, -1, "%s", cudaGetErrorString(e));
+    if (prop.major != 10 || prop.minor != 0)
+        return set_error(MFFT_ERR_LIBRARY_BUILD, -1, -1, -1,
+                         "libmfft is built for sm_100a only; device %d is sm_%d%d (%s)", device,
+                         prop.major, prop.minor, prop.name);
+    DeviceGuard g(device);
+    mfft_ctx* c = new mfft_ctx();
+    c->device = device;
+    c->sms = prop.multiProcessorCount;
+    c->l2_bytes = prop.l2CacheSize;
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return set_error(MFFT_ERR_NO_STREAM, -1, -1, -1, "Could not create CUDA stream: %s",
+                         cudaGetErrorString(e));
+    }
+    *out = c;
+    return MFFT_SUCCESS;
+}
+
+static std::mutex g_shared_mu;
+static mfft_ctx* g_shared[64];
+
+extern "C" int mfft_context_shared(mfft_ctx** out) {
+    if (!out) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "out is NULL");
+    int dev = 0;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return set_error(MFFT_ERR_NO_DEVICE, -1, -1, -1, "No CUDA device available");
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return set_error(MFFT_ERR_NO_DEVICE, -1, -1, -1, "device %d", dev);
+    std::lock_guard<std::mutex> lk(g_shared_mu);
+    if (!g_shared[dev]) {
+        mfft_ctx* c = nullptr;
+        int st = ctx_init(dev, &c);
+        if (st) return st;
+        c->shared = true;
+        g_shared[dev] = c;
+    }
+    *out = g_shared[dev];
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_context_create(int device, mfft_ctx** out) {
+    if (!out) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "out is NULL");
+    return ctx_init(device, out);
+}
+
+extern "C" int mfft_context_destroy(mfft_ctx* ctx) {
+    if (!ctx) return MFFT_SUCCESS;
+    if (ctx->shared)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "the shared context is never destroyed");
+    DeviceGuard g(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->twiddles) cudaFree(kv.second);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_context_sm_count(const mfft_ctx* ctx) { return ctx ? ctx->sms : 0; }
+
+namespace mfft {
+
+// Twiddle rows of a (kernel n, e) pair, built once per context on the device.
+int ctx_twiddles(mfft_ctx* ctx, const BatchedKernel* k, float2** out) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto key = std::make_pair(k->n, k->e);
+    auto it = ctx->twiddles.find(key);
+    if (it != ctx->twiddles.end()) {
+        *out = it->second;
+        return MFFT_SUCCESS;
+    }
+    float2* tw = nullptr;
+    cudaError_t e = cudaMalloc(&tw, sizeof(float2) * (size_t)k->tw_size);
+    if (e != cudaSuccess) return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "twiddle table: %s", cudaGetErrorString(e));
+    k->gen_twiddles(tw, ctx->stream);
+    e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaFree(tw);
+        return cuda_error(e, "twiddle generation");
+    }
+    ctx->twiddles[key] = tw;
+    *out = tw;
+    return MFFT_SUCCESS;
+}
+
+int bind_batched(mfft_ctx* ctx, const BatchedKernel* k, BatchedBinding* b) {
+    cudaError_t e = k->prepare();
+    if (e != cudaSuccess) return cuda_error(e, "kernel attributes");
+    b->k = k;
+    return ctx_twiddles(ctx, k, &b->tw);
+}
+
+}  // namespace mfft
+
+// ---------------------------------------------------------------------------
+// plans
+// ---------------------------------------------------------------------------
+
+extern "C" int64_t mfft_recommended_fft_size(int64_t kernel_count) {
+    static const int64_t sizes[] = {64, 128, 256, 512, 1024, 2048, 4096, 8192, 16384};
+    for (int64_t s : sizes)
+        if (s > kernel_count) return s;
+    return 0;
+}
+
+extern "C" int mfft_plan_create(mfft_ctx* ctx, int64_t n, mfft_plan** out) {
+    if (!out) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "out is NULL");
+    *out = nullptr;
+    if (!ctx) {
+        int st = mfft_context_shared(&ctx);
+        if (st) return st;
+    }
+    if (!is_pow2_in(n, 64, MFFT_MAX_N))
+        return set_error(MFFT_ERR_UNSUPPORTED_SIZE, n, -1, -1,
+                         "Unsupported FFT size: %lld. Supported: powers of two 64..%d", (long long)n,
+                         MFFT_MAX_N);
+    DeviceGuard g(ctx->device);
+    mfft_plan* p = new mfft_plan();
+    p->ctx = ctx;
+    p->n = n;
+    int st = MFFT_SUCCESS;
+    if (n <= MFFT_MAX_SINGLE_N) {
+        const BatchedKernel* k = tuned_batched(ctx, (int)n);
+        if (!k) {
+            delete p;
+            return set_error(MFFT_ERR_KERNEL_NOT_FOUND, -1, -1, -1, "no batched kernel for n=%lld", (long long)n);
+        }
+        st = bind_batched(ctx, k, &p->line);
+    } else {
+        st = fourstep_plan_init(p);
+    }
+    if (st) {
+        mfft_plan_destroy(p);
+        return st;
+    }
+    *out = p;
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_plan_destroy(mfft_plan* plan) {
+    if (!plan) return MFFT_SUCCESS;
+    DeviceGuard g(plan->ctx->device);
+    fourstep_plan_release(plan);
+    tc_plan_release(plan);
+    delete plan;
+    return MFFT_SUCCESS;
+}
+
+extern "C" int64_t mfft_plan_size(const mfft_plan* plan) { return plan ? plan->n : 0; }
+
+// ---------------------------------------------------------------------------
+// execution
+// ---------------------------------------------------------------------------
+
+namespace mfft {
+
+int launch_c2c_device(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,
+                      cudaStream_t s) {
+    cudaError_t e;
+    if (plan->n <= MFFT_MAX_SINGLE_N) {
+        const BatchedKernel* k = plan->line.k;
+        e = (direction == MFFT_INVERSE ? k->inv : k->fwd)(in, out, batch, plan->line.tw, s);
+        if (e != cudaSuccess) return cuda_error(e, "batched FFT launch");
+        return MFFT_SUCCESS;
+    }
+    return fourstep_exec(plan, in, out, batch, direction, s);
+}
+
+int check_exec_args(const void* in, void* out, int64_t batch, int direction, int flags) {
+    if (batch < 0) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, batch, -1, "batch must be >= 0, got %lld", (long long)batch);
+    if (direction != MFFT_FORWARD && direction != MFFT_INVERSE)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "direction must be -1 or +1, got %d", direction);
+    if (flags != MFFT_HOST_MEMORY && flags != MFFT_DEVICE_MEMORY)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "unknown flags %d", flags);
+    if (batch > 0 && (!in || !out)) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "NULL buffer");
+    return MFFT_SUCCESS;
+}
+
+// Host-array call: stage through one device buffer on the context stream and
+// wait, like MetalFFT's copy-in / commitAndWait / copy-out.
+int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, size_t out_bytes,
+                    const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body) {
+    cudaStream_t s = ctx->stream;
+    void* d_in = nullptr;
+    void* d_out = nullptr;
+    cudaError_t e = cudaMallocAsync(&d_in, in_bytes ? in_bytes : 16, s);
+    if (e != cudaSuccess) return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "Device buffer allocation failed: %s", cudaGetErrorString(e));
+    bool same = (in_bytes == out_bytes);
+    if (same) {
+        d_out = d_in;
+    } else {
+        e = cudaMallocAsync(&d_out, out_bytes ? out_bytes : 16, s);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(d_in, s);
+            cudaStreamSynchronize(s);
+            return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "Device buffer allocation failed: %s", cudaGetErrorString(e));
+        }
+    }
+    int st = MFFT_SUCCESS;
+    if (in_bytes) e = cudaMemcpyAsync(d_in, in, in_bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) st = cuda_error(e, "host to device copy");
+    if (!st) st = body(d_in, d_out, s);
+    if (!st && out_bytes) {
+        e = cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) st = cuda_error(e, "device to host copy");
+    }
+    cudaFreeAsync(d_in, s);
+    if (!same) cudaFreeAsync(d_out, s);
+    e = cudaStreamSynchronize(s);
+    if (!st && e != cudaSuccess) st = cuda_error(e, "execution");
+    return st;
+}
+
+}  // namespace mfft
+
+extern "C" int mfft_exec_c2c(mfft_plan* plan, const void* in, void* out, int64_t batch, int direction,
+                             int flags, void* stream) {
+    if (!plan) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "plan is NULL");
+    int st = check_exec_args(in, out, batch, direction, flags);
+    if (st) return st;
+    if (batch == 0) return MFFT_SUCCESS;
+    DeviceGuard g(plan->ctx->device);
+    if (flags == MFFT_DEVICE_MEMORY)
+        return launch_c2c_device(plan, (const float2*)in, (float2*)out, batch, direction,
+                                 (cudaStream_t)stream);
+    size_t bytes = (size_t)batch * (size_t)plan->n * sizeof(float2);
+    return run_host_staged(plan->ctx, in, out, bytes, bytes, [&](void* di, void* dout, cudaStream_t s) {
+        return launch_c2c_device(plan, (const float2*)di, (float2*)dout, batch, direction, s);
+    });
+}

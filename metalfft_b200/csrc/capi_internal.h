@@ -1,0 +1,92 @@
+// capi_internal.h -- handle layouts and helpers shared by the C-ABI sources.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <functional>
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "../../include/mfft.h"
+#include "kernels.h"
+
+#define MFFT_MAX_N (1 << 20)
+#define MFFT_MAX_SINGLE_N 16384
+
+struct mfft_ctx {
+    int device = 0;
+    int sms = 0;
+    int l2_bytes = 0;
+    bool shared = false;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::map<std::pair<int, int>, float2*> twiddles;     // (n, e) -> twiddle rows
+    std::map<int, const mfft::BatchedKernel*> tuned;     // n -> autotuned kernel
+};
+
+namespace mfft {
+
+struct BatchedBinding {
+    const BatchedKernel* k = nullptr;
+    float2* tw = nullptr;
+};
+
+// Four-step state for n > 16384 (n = n1 * n2, both <= 16384).
+struct FourStep {
+    int n1 = 0, n2 = 0;
+    const void* col = nullptr;   // column-pass kernel descriptor
+    const void* row = nullptr;   // row-pass kernel descriptor
+    float2* col_tw = nullptr;
+    float2* row_tw = nullptr;
+    float2* tables = nullptr;    // W_N^m = fine[m % 1024] * coarse[m / 1024]
+    float2* scratch = nullptr;   // intermediate, scratch_lines * n float2
+    long long scratch_lines = 0;
+};
+
+struct TcState {
+    void* dft_tables = nullptr;  // device: realified DFT16 operands (hi/lo, bf16)
+    float2* tw = nullptr;        // device: inter-stage twiddles
+    bool ready = false;
+};
+
+}  // namespace mfft
+
+struct mfft_plan {
+    mfft_ctx* ctx = nullptr;
+    int64_t n = 0;
+    mfft::BatchedBinding line;
+    mfft::FourStep fs;
+    mfft::TcState tc;
+};
+
+namespace mfft {
+
+int set_error(int status, int64_t expected, int64_t got, int64_t index, const char* fmt, ...);
+int cuda_error(cudaError_t e, const char* what);
+bool is_pow2_in(int64_t n, int64_t lo, int64_t hi);
+
+struct DeviceGuard {
+    explicit DeviceGuard(int dev);
+    ~DeviceGuard();
+    int prev_ = 0;
+};
+
+int ctx_twiddles(mfft_ctx* ctx, const BatchedKernel* k, float2** out);
+int bind_batched(mfft_ctx* ctx, const BatchedKernel* k, BatchedBinding* b);
+const BatchedKernel* tuned_batched(mfft_ctx* ctx, int n);
+
+int check_exec_args(const void* in, void* out, int64_t batch, int direction, int flags);
+int launch_c2c_device(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,
+                      cudaStream_t s);
+int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, size_t out_bytes,
+                    const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body);
+
+int fourstep_plan_init(mfft_plan* plan);
+void fourstep_plan_release(mfft_plan* plan);
+int fourstep_exec(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,
+                  cudaStream_t s);
+
+void tc_plan_release(mfft_plan* plan);
+
+}  // namespace mfft

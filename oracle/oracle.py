@@ -1,0 +1,177 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() (as the
+checker) and bench.py's CPU-baseline leg.  The product (metalfft_b200/) never
+imports it.  See oracle.c for what each function restates.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+_i64, _int, _dbl = ctypes.c_int64, ctypes.c_int, ctypes.c_double
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "mfo_max_threads": (_int, []),
+            "mfo_dft_c128": (None, [_dp, _dp, _i64, _int]),
+            "mfo_fft_c128": (None, [_dp, _dp, _i64, _i64, _int, _int]),
+            "mfo_fft_c64_to_c128": (None, [_fp, _dp, _i64, _i64, _int, _int]),
+            "mfo_rel_rms_c64_vs_c128": (_dbl, [_fp, _dp, _i64, _int]),
+            "mfo_ref_fft_c64": (None, [_fp, _fp, _int, _i64, _int, _int]),
+            "mfo_ref_fourstep_split": (None, [_int, ctypes.POINTER(_int), ctypes.POINTER(_int)]),
+            "mfo_ref_conv_ola_f32": (None, [_fp, _i64, _fp, _int, _int, _fp, _int]),
+            "mfo_conv_f64": (None, [_dp, _i64, _dp, _int, _int, _dp, _int]),
+            "mfo_conv_adjoint_f64": (None, [_dp, _i64, _dp, _int, _dp, _dp, _dp]),
+            "mfo_corr_f64": (None, [_dp, _i64, _dp, _i64, _int, _dp]),
+            "mfo_ref_corr_f32": (None, [_fp, _i64, _fp, _i64, _int, _fp]),
+            "mfo_window": (None, [_int, _int, _dbl, _dp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _f(a):
+    return a.ctypes.data_as(_fp)
+
+
+def max_threads():
+    return load().mfo_max_threads()
+
+
+def dft(x, sign=-1):
+    """Naive FP64 DFT of one line (exact index reduction)."""
+    x = np.ascontiguousarray(x, np.complex128)
+    out = np.empty_like(x)
+    load().mfo_dft_c128(_d(x), _d(out), x.size, sign)
+    return out
+
+
+def fft64(x, sign=-1, threads=0):
+    """FP64 FFT of each row of x (complex128), unscaled."""
+    x = np.ascontiguousarray(x, np.complex128)
+    n = x.shape[-1]
+    out = np.empty_like(x)
+    load().mfo_fft_c128(_d(x), _d(out), n, x.size // n, sign, threads)
+    return out
+
+
+def truth(x64, inverse=False, threads=0):
+    """FP64 ground truth for complex64 rows: forward, or inverse with 1/n."""
+    x64 = np.ascontiguousarray(x64, np.complex64)
+    n = x64.shape[-1]
+    out = np.empty(x64.shape, np.complex128)
+    load().mfo_fft_c64_to_c128(_f(x64), _d(out), n, x64.size // n, +1 if inverse else -1, threads)
+    if inverse:
+        out /= n
+    return out
+
+
+def rel_rms(y, ref, threads=0):
+    """||y - ref|| / ||ref|| in FP64 (MetalFFTTests.swift:190-198 definition)."""
+    y = np.ascontiguousarray(y, np.complex64)
+    ref = np.ascontiguousarray(ref, np.complex128)
+    return load().mfo_rel_rms_c64_vs_c128(_f(y), _d(ref), y.size, threads)
+
+
+def ref_fft(x, inverse=False, threads=0):
+    """FP32 restatement of the reference's Stockham / four-step path."""
+    x = np.ascontiguousarray(x, np.complex64)
+    n = x.shape[-1]
+    out = np.empty_like(x)
+    load().mfo_ref_fft_c64(_f(x), _f(out), n, x.size // n, 1 if inverse else 0, threads)
+    return out
+
+
+def ref_fourstep_split(n):
+    a, b = _int(), _int()
+    load().mfo_ref_fourstep_split(n, ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
+
+
+def ref_conv(x, h, fft, threads=0):
+    x = np.ascontiguousarray(x, np.float32)
+    h = np.ascontiguousarray(h, np.float32)
+    y = np.empty(len(x) + len(h) - 1, np.float32)
+    load().mfo_ref_conv_ola_f32(_f(x), len(x), _f(h), len(h), fft, _f(y), threads)
+    return y
+
+
+def conv64(x, h, fft, threads=0):
+    x = np.ascontiguousarray(x, np.float64)
+    h = np.ascontiguousarray(h, np.float64)
+    y = np.empty(len(x) + len(h) - 1, np.float64)
+    load().mfo_conv_f64(_d(x), len(x), _d(h), len(h), fft, _d(y), threads)
+    return y
+
+
+def conv_adjoint64(x, h, g):
+    x = np.ascontiguousarray(x, np.float64)
+    h = np.ascontiguousarray(h, np.float64)
+    g = np.ascontiguousarray(g, np.float64)
+    dx = np.empty(len(x), np.float64)
+    dh = np.empty(len(h), np.float64)
+    load().mfo_conv_adjoint_f64(_d(x), len(x), _d(h), len(h), _d(g), _d(dx), _d(dh))
+    return dx, dh
+
+
+def corr64(a, b, fft):
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    r = np.empty(fft, np.float64)
+    load().mfo_corr_f64(_d(a), len(a), _d(b), len(b), fft, _d(r))
+    return r
+
+
+def ref_corr(a, b, fft):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    r = np.empty(fft, np.float32)
+    load().mfo_ref_corr_f32(_f(a), len(a), _f(b), len(b), fft, _f(r))
+    return r
+
+
+def window(kind, n, beta=6.0):
+    w = np.empty(n, np.float64)
+    load().mfo_window(kind, n, beta, _d(w))
+    return w
+
+
+# ---- seeded generators shared by tests, smoke and bench ---------------------
+
+def uniform_c64(shape, seed, lo=-1.0, hi=1.0):
+    """re, im i.i.d. U[lo, hi) (the reference's Float.random(in: -1...1))."""
+    rng = np.random.default_rng(seed)
+    z = rng.uniform(lo, hi, size=tuple(shape) + (2,)).astype(np.float32)
+    return z.view(np.complex64)[..., 0]
+
+
+def normal_c64(shape, seed):
+    rng = np.random.default_rng(seed)
+    z = rng.standard_normal(size=tuple(shape) + (2,), dtype=np.float32)
+    return z.view(np.complex64)[..., 0]

@@ -1,0 +1,179 @@
+"""Parity of the CUDA batched FFT (through libmfft's C ABI) with the FP64
+oracle, following the reference's own tests (Tests/MetalFFTTests/
+MetalFFTTests.swift) with tighter bars: FP32 <= 2e-6 rel RMS for N <= 16384
+against FP64 (the reference: 1e-4 against vDSP), 3e-6 for the four-step sizes."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [64, 128, 256, 512, 1024, 2048, 4096, 8192, 16384]
+BIG = [1 << 15, 1 << 16, 1 << 17, 1 << 18, 1 << 19, 1 << 20]
+TOL = 2e-6       # FP32, N <= 16384, rel RMS vs FP64
+TOL_BIG = 3e-6   # four-step sizes
+
+
+@pytest.fixture(scope="module")
+def M():
+    import metalfft_b200
+    return metalfft_b200
+
+
+def tol(n):
+    return TOL if n <= 16384 else TOL_BIG
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_all_sizes_impulse(M, n):
+    # MetalFFTTests.swift:11-23
+    x = np.zeros(n, np.complex64)
+    x[0] = 1
+    y = M.MetalFFT(n).forward(x)
+    assert np.max(np.abs(y.real - 1)) < 1e-6 and np.max(np.abs(y.imag)) < 1e-6
+
+
+@pytest.mark.parametrize("n", SIZES + BIG)
+def test_random_vs_fp64(M, n):
+    # MetalFFTTests.swift:25-35, against FP64 instead of vDSP
+    b = 3 if n <= 16384 else 2
+    x = O.uniform_c64((b, n), seed=1000 + n)
+    f = M.MetalFFT(n)
+    y = f.forward_batch(x)
+    assert O.rel_rms(y, O.truth(x)) < tol(n)
+    xi = f.inverse_batch(x)
+    assert O.rel_rms(xi, O.truth(x, inverse=True)) < tol(n)
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_every_registered_variant(M, n):
+    x = O.normal_c64((5, n), seed=2000 + n)
+    ref = O.truth(x)
+    f = M.MetalFFT(n)
+    for radix, fpb in M.MetalFFT.variants(n):
+        f.set_kernel(radix, fpb)
+        assert O.rel_rms(f.forward_batch(x), ref) < TOL, (radix, fpb)
+
+
+@pytest.mark.parametrize("n", [64, 4096, 16384, 1 << 20])
+def test_round_trip(M, n):
+    x = O.uniform_c64((2, n), seed=3000 + n)
+    f = M.MetalFFT(n)
+    z = f.inverse_batch(f.forward_batch(x))
+    assert O.rel_rms(z, x.astype(np.complex128)) < 2 * tol(n)
+
+
+def test_single_matches_batch_bitwise(M):
+    # MetalFFTTests.swift:51-65 (the reference allows 1e-4; same kernel here)
+    n = 512
+    x = O.uniform_c64((2, n), seed=4)
+    f = M.MetalFFT(n)
+    yb = f.forward_batch([x[0], x[1]])
+    assert np.array_equal(yb[0], f.forward(x[0]))
+    assert np.array_equal(yb[1], f.forward(x[1]))
+
+
+def test_cosine_peak_bin(M):
+    # MetalFFTTests.swift:37-49
+    n = 1024
+    k = np.arange(n)
+    x = np.cos(2 * np.pi * 100 * k / n).astype(np.complex64)
+    y = M.MetalFFT(n).forward(x)
+    assert int(np.argmax(np.abs(y[: n // 2]) ** 2)) == 100
+
+
+def test_golden_fixtures(M):
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "fft_golden.npz"))
+    for n in [64, 512, 4096]:
+        y = M.MetalFFT(n).forward_batch(z["x_%d" % n])
+        assert O.rel_rms(y, z["X_%d" % n]) < TOL
+
+
+def test_forward_into_and_multichannel(M):
+    n = 256
+    x = O.uniform_c64((4, n), seed=9)
+    f = M.MetalFFT(n)
+    out = np.zeros(3, np.complex64)
+    f.forward_into(x[0], out)
+    assert out.shape == (n,) and O.rel_rms(out[None], O.truth(x[:1])) < TOL
+    mc = M.MultiChannelFFT(4, n)
+    assert O.rel_rms(mc.forward(x), O.truth(x)) < TOL
+    assert O.rel_rms(mc.inverse(x), O.truth(x, inverse=True)) < TOL
+    with pytest.raises(M.FFTError):
+        mc.forward(x[:3])
+
+
+def test_device_tensors_and_in_place(M):
+    import torch
+    n = 4096
+    x = O.normal_c64((64, n), seed=10)
+    f = M.MetalFFT(n)
+    t = torch.from_numpy(x).cuda()
+    y = f.forward_batch(t)
+    assert y.is_cuda
+    assert O.rel_rms(y.cpu().numpy(), O.truth(x)) < TOL
+    f.exec(t, t, 64)  # in place
+    torch.cuda.synchronize()
+    assert np.array_equal(t.cpu().numpy(), y.cpu().numpy())
+
+
+def test_errors_mirror_fft_error(M):
+    with pytest.raises(M.FFTError) as e:
+        M.MetalFFT(100)
+    assert e.value.case == "unsupportedFFTSize" and e.value.expected == 100
+    for bad in [32, 3 << 10, 1 << 21]:
+        with pytest.raises(M.FFTError):
+            M.MetalFFT(bad)
+    f = M.MetalFFT(256)
+    with pytest.raises(M.FFTError) as e:
+        f.forward(np.zeros(255, np.complex64))
+    assert e.value.case == "invalidInputSize" and (e.value.expected, e.value.got) == (256, 255)
+    with pytest.raises(M.FFTError) as e:
+        f.forward_batch([np.zeros(256, np.complex64), np.zeros(200, np.complex64)])
+    assert e.value.case == "batchInputSize" and e.value.batch_index == 1
+    assert f.forward_batch([]).shape == (0, 256)
+
+
+def test_config1_batch256_forward_inverse(M):
+    """N=4096, batch 256, U[-1,1): forward, inverse, round trip vs FP64."""
+    n, b = 4096, 256
+    x = O.uniform_c64((b, n), seed=12345)
+    f = M.MetalFFT(n)
+    X = f.forward_batch(x)
+    assert O.rel_rms(X, O.truth(x)) < TOL
+    xr = f.inverse_batch(X)
+    assert O.rel_rms(xr, x.astype(np.complex128)) < TOL
+
+
+def test_config3_full_batch_properties(M):
+    """N=4096 x 16384 (512 MiB): sampled rows vs FP64, and linearity of the
+    whole batch (a size-independent property)."""
+    import torch
+    n, b = 4096, 16384
+    g = torch.Generator(device="cuda").manual_seed(7)
+    x = torch.randn(b, n, dtype=torch.complex64, device="cuda", generator=g)
+    yv = torch.randn(b, n, dtype=torch.complex64, device="cuda", generator=g)
+    f = M.MetalFFT(n)
+    X = f.forward_batch(x)
+    Y = f.forward_batch(yv)
+    rows = torch.randint(0, b, (32,), generator=torch.Generator().manual_seed(1))
+    xs = x[rows].cpu().numpy()
+    assert O.rel_rms(X[rows].cpu().numpy(), O.truth(xs)) < TOL
+    Z = f.forward_batch(x + 2 * yv)
+    lin = torch.linalg.vector_norm(Z - (X + 2 * Y)) / torch.linalg.vector_norm(Z)
+    assert float(lin) < 4e-7 * 10
+    # last rows (tail of the grid)
+    assert O.rel_rms(X[-3:].cpu().numpy(), O.truth(x[-3:].cpu().numpy())) < TOL
+
+
+def test_autotune_picks_a_registered_variant(M):
+    import ctypes
+    r, fpb = ctypes.c_int(), ctypes.c_int()
+    st = M.lib.mfft_autotune(M.shared_context(), 1024, 4096, ctypes.byref(r), ctypes.byref(fpb))
+    assert st == 0 and (r.value, fpb.value) in M.MetalFFT.variants(1024)
+    f = M.MetalFFT(1024)
+    assert (f.kernel_info["radix"], f.kernel_info["lines_per_cta"]) == (r.value, fpb.value)
+    x = O.normal_c64((3, 1024), seed=77)
+    assert O.rel_rms(f.forward_batch(x), O.truth(x)) < TOL
