@@ -116,6 +116,10 @@ MFFT_API int mfft_context_create(int device, mfft_ctx** out);
 MFFT_API int mfft_context_destroy(mfft_ctx* ctx);
 /* Number of SMs of the context's device (grid sizing). */
 MFFT_API int mfft_context_sm_count(const mfft_ctx* ctx);
+/* Waits for the device and reports MFFT_ERR_TIMEOUT if any kernel of this
+ * context gave up a bounded device-side wait since the last check (host-array
+ * calls check after every call; device-pointer calls are checked here). */
+MFFT_API int mfft_context_check(mfft_ctx* ctx);
 
 /* ---- plans: MetalFFT.init(size:) (MetalFFT.swift:27-51) ---------------- */
 
@@ -129,21 +133,27 @@ MFFT_API int64_t mfft_plan_size(const mfft_plan* plan);
  * size list, or 0 (Convolver.recommendedFFTSize, Convolve.swift:83-86). */
 MFFT_API int64_t mfft_recommended_fft_size(int64_t kernel_count);
 
-/* Autotuner (no reference counterpart; the reference hard-codes one kernel
- * per size, MetalContext.swift:47-69): times every registered radix /
- * lines-per-CTA variant of the batched kernel for size n (64..16384) over
- * `lines` lines (<= 0: 256 MiB worth) and keeps the fastest for this context;
- * appends "n radix lines_per_cta" to the file named by $MFFT_TUNE_CACHE, which
- * later plans read.  Reports the choice. */
-MFFT_API int mfft_autotune(mfft_ctx* ctx, int64_t n, int64_t lines, int* radix, int* lines_per_cta);
-/* Pins a plan (n <= 16384) to one registered variant: main radix 8 or 16 and
- * lines per CTA.  MFFT_ERR_KERNEL_NOT_FOUND if that variant is not built. */
-MFFT_API int mfft_plan_set_kernel(mfft_plan* plan, int radix, int lines_per_cta);
-/* Lists the registered variants for size n: fills up to cap (radix,
- * lines_per_cta) pairs and returns how many exist (host only). */
-MFFT_API int mfft_list_kernels(int64_t n, int* radix, int* lines_per_cta, int cap);
-/* The kernel a plan uses: main radix, lines per CTA, threads per CTA. */
-MFFT_API int mfft_plan_kernel_info(const mfft_plan* plan, int* radix, int* lines_per_cta, int* threads);
+/* Batched-kernel variants.  A variant of size n is (radix, lines_per_cta,
+ * stages): main radix 8 or 16, lines transformed per CTA, and stages = 0 for
+ * the direct-load kernel or the number of line groups a persistent CTA keeps
+ * in flight with TMA bulk copies.
+ *
+ * Autotuner (no reference counterpart; the reference hard-codes one kernel
+ * per size, MetalContext.swift:47-69): times every registered variant for
+ * size n (64..16384) over `lines` lines (<= 0: 256 MiB worth) and keeps the
+ * fastest for this context; appends "n radix lines_per_cta stages" to the file
+ * named by $MFFT_TUNE_CACHE, which later contexts read.  Reports the choice. */
+MFFT_API int mfft_autotune(mfft_ctx* ctx, int64_t n, int64_t lines, int* radix, int* lines_per_cta,
+                           int* stages);
+/* Pins a plan (n <= 16384) to one registered variant.
+ * MFFT_ERR_KERNEL_NOT_FOUND if that variant is not built. */
+MFFT_API int mfft_plan_set_kernel(mfft_plan* plan, int radix, int lines_per_cta, int stages);
+/* Lists the registered variants for size n: fills up to cap entries and
+ * returns how many exist (host only). */
+MFFT_API int mfft_list_kernels(int64_t n, int* radix, int* lines_per_cta, int* stages, int cap);
+/* The variant a plan uses and its threads per CTA. */
+MFFT_API int mfft_plan_kernel_info(const mfft_plan* plan, int* radix, int* lines_per_cta, int* threads,
+                                   int* stages);
 
 /* ---- execution --------------------------------------------------------- */
 

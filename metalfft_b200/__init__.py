@@ -120,25 +120,28 @@ class MetalFFT:
 
     def __del__(self):
         p = getattr(self, "_plan", None)
-        if p:
+        if p and lib is not None:
             lib.mfft_plan_destroy(p)
             self._plan = None
 
     @property
     def kernel_info(self):
-        r, f, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        _check(lib.mfft_plan_kernel_info(self._plan, ctypes.byref(r), ctypes.byref(f), ctypes.byref(t)))
-        return {"radix": r.value, "lines_per_cta": f.value, "threads": t.value}
+        r, f, t, s = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib.mfft_plan_kernel_info(self._plan, ctypes.byref(r), ctypes.byref(f), ctypes.byref(t),
+                                         ctypes.byref(s)))
+        return {"radix": r.value, "lines_per_cta": f.value, "threads": t.value, "stages": s.value}
 
-    def set_kernel(self, radix, lines_per_cta):
-        _check(lib.mfft_plan_set_kernel(self._plan, radix, lines_per_cta))
+    def set_kernel(self, radix, lines_per_cta, stages=0):
+        _check(lib.mfft_plan_set_kernel(self._plan, radix, lines_per_cta, stages))
 
     @staticmethod
     def variants(n):
+        """Registered (radix, lines_per_cta, stages) variants for size n."""
         r = (ctypes.c_int * 64)()
         f = (ctypes.c_int * 64)()
-        m = lib.mfft_list_kernels(n, r, f, 64)
-        return [(r[i], f[i]) for i in range(min(m, 64))]
+        s = (ctypes.c_int * 64)()
+        m = lib.mfft_list_kernels(n, r, f, s, 64)
+        return [(r[i], f[i], s[i]) for i in range(min(m, 64))]
 
     # ---- raw entry ---------------------------------------------------------
     def exec(self, inp, out, batch, direction=FORWARD, tc_variant=0):

@@ -52,7 +52,7 @@ class Convolver:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:
             lib.mfft_conv_destroy(h)
             self._h = None
 
@@ -124,7 +124,7 @@ class Correlator:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:
             lib.mfft_corr_destroy(h)
             self._h = None
 
@@ -203,7 +203,7 @@ class FFTAnalyzer:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:
             lib.mfft_analyzer_destroy(h)
             self._h = None
 
@@ -243,7 +243,7 @@ class MixedBatch:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:
             lib.mfft_multi_destroy(h)
             self._h = None
 

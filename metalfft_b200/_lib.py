@@ -25,14 +25,15 @@ SIGNATURES = [
     ("mfft_context_create", c_int, [c_int, P(c_void_p)]),
     ("mfft_context_destroy", c_int, [c_void_p]),
     ("mfft_context_sm_count", c_int, [c_void_p]),
+    ("mfft_context_check", c_int, [c_void_p]),
     ("mfft_plan_create", c_int, [c_void_p, c_int64, P(c_void_p)]),
     ("mfft_plan_destroy", c_int, [c_void_p]),
     ("mfft_plan_size", c_int64, [c_void_p]),
     ("mfft_recommended_fft_size", c_int64, [c_int64]),
-    ("mfft_autotune", c_int, [c_void_p, c_int64, c_int64, P(c_int), P(c_int)]),
-    ("mfft_plan_kernel_info", c_int, [c_void_p, P(c_int), P(c_int), P(c_int)]),
-    ("mfft_plan_set_kernel", c_int, [c_void_p, c_int, c_int]),
-    ("mfft_list_kernels", c_int, [c_int64, P(c_int), P(c_int), c_int]),
+    ("mfft_autotune", c_int, [c_void_p, c_int64, c_int64, P(c_int), P(c_int), P(c_int)]),
+    ("mfft_plan_kernel_info", c_int, [c_void_p, P(c_int), P(c_int), P(c_int), P(c_int)]),
+    ("mfft_plan_set_kernel", c_int, [c_void_p, c_int, c_int, c_int]),
+    ("mfft_list_kernels", c_int, [c_int64, P(c_int), P(c_int), P(c_int), c_int]),
     ("mfft_exec_c2c", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),
     ("mfft_exec_c2c_tc", c_int,
      [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p]),

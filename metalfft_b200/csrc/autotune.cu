@@ -6,7 +6,7 @@
 // batches switch to the radix-8 kernel, MetalFFT.swift:163-165).  Here every
 // registered instantiation for the size is timed with CUDA events on a batch
 // larger than L2 and the fastest is kept.  The cache file (one line
-// "n e fpb" per size) is read from $MFFT_TUNE_CACHE when that is set.
+// "n e fpb stages" per size) is read from $MFFT_TUNE_CACHE when that is set.
 #include <stdio.h>
 #include <stdlib.h>
 
@@ -16,17 +16,18 @@
 
 namespace mfft {
 
-static bool read_cache(int n, int* e, int* fpb) {
+static bool read_cache(int n, int* e, int* fpb, int* st) {
     const char* path = getenv("MFFT_TUNE_CACHE");
     if (!path || !*path) return false;
     FILE* f = fopen(path, "r");
     if (!f) return false;
-    int cn, ce, cf;
+    int cn, ce, cf, cs;
     bool found = false;
-    while (fscanf(f, "%d %d %d", &cn, &ce, &cf) == 3) {
+    while (fscanf(f, "%d %d %d %d", &cn, &ce, &cf, &cs) == 4) {
         if (cn == n) {
             *e = ce;
             *fpb = cf;
+            *st = cs;
             found = true;
         }
     }
@@ -34,12 +35,12 @@ static bool read_cache(int n, int* e, int* fpb) {
     return found;
 }
 
-static void write_cache(int n, int e, int fpb) {
+static void write_cache(int n, int e, int fpb, int st) {
     const char* path = getenv("MFFT_TUNE_CACHE");
     if (!path || !*path) return;
     FILE* f = fopen(path, "a");
     if (!f) return;
-    fprintf(f, "%d %d %d\n", n, e, fpb);
+    fprintf(f, "%d %d %d %d\n", n, e, fpb, st);
     fclose(f);
 }
 
@@ -50,8 +51,8 @@ const BatchedKernel* tuned_batched(mfft_ctx* ctx, int n) {
         if (it != ctx->tuned.end()) return it->second;
     }
     const BatchedKernel* k = nullptr;
-    int e = 0, fpb = 0;
-    if (read_cache(n, &e, &fpb)) k = find_batched(n, e, fpb);
+    int e = 0, fpb = 0, st = 0;
+    if (read_cache(n, &e, &fpb, &st)) k = find_batched(n, e, fpb, st);
     if (!k) k = default_batched(n);
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->tuned[n] = k;
@@ -80,10 +81,11 @@ int autotune_batched(mfft_ctx* ctx, int n, long long lines, const BatchedKernel*
         if (ks[i].n != n) continue;
         BatchedBinding bb;
         if (bind_batched(ctx, &ks[i], &bb) != MFFT_SUCCESS) continue;
-        for (int w = 0; w < 3; ++w) ks[i].fwd(a, b, lines, bb.tw, ctx->stream);
+        for (int w = 0; w < 3; ++w) ks[i].fwd(a, b, lines, bb.tw, ctx->dev_err, ctx->stream);
         cudaEventRecord(e0, ctx->stream);
         const int reps = 10;
-        for (int r = 0; r < reps; ++r) ks[i].fwd((r & 1) ? b : a, (r & 1) ? a : b, lines, bb.tw, ctx->stream);
+        for (int r = 0; r < reps; ++r)
+            ks[i].fwd((r & 1) ? b : a, (r & 1) ? a : b, lines, bb.tw, ctx->dev_err, ctx->stream);
         cudaEventRecord(e1, ctx->stream);
         if (cudaEventSynchronize(e1) != cudaSuccess) continue;
         float ms = 0.f;
@@ -104,14 +106,15 @@ int autotune_batched(mfft_ctx* ctx, int n, long long lines, const BatchedKernel*
         std::lock_guard<std::mutex> lk(ctx->mu);
         ctx->tuned[n] = best;
     }
-    write_cache(n, best->e, best->fpb);
+    write_cache(n, best->e, best->fpb, best->stages);
     *out = best;
     return MFFT_SUCCESS;
 }
 
 }  // namespace mfft
 
-extern "C" int mfft_autotune(mfft_ctx* ctx, int64_t n, int64_t lines, int* radix, int* lines_per_cta) {
+extern "C" int mfft_autotune(mfft_ctx* ctx, int64_t n, int64_t lines, int* radix, int* lines_per_cta,
+                             int* stages) {
     using namespace mfft;
     if (!ctx) {
         int st = mfft_context_shared(&ctx);
@@ -125,32 +128,36 @@ extern "C" int mfft_autotune(mfft_ctx* ctx, int64_t n, int64_t lines, int* radix
     if (st) return st;
     if (radix) *radix = k->e;
     if (lines_per_cta) *lines_per_cta = k->fpb;
-    return MFFT_SUCCESS;
+    if (stages) *stages = k->stages;
+    return check_device_error(ctx);
 }
 
-extern "C" int mfft_plan_kernel_info(const mfft_plan* plan, int* radix, int* lines_per_cta, int* threads) {
+extern "C" int mfft_plan_kernel_info(const mfft_plan* plan, int* radix, int* lines_per_cta, int* threads,
+                                     int* stages) {
     if (!plan) return mfft::set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "plan is NULL");
     const mfft::BatchedKernel* k = plan->line.k;
     if (radix) *radix = k ? k->e : 16;
     if (lines_per_cta) *lines_per_cta = k ? k->fpb : 0;
     if (threads) *threads = k ? k->threads : 0;
+    if (stages) *stages = k ? k->stages : 0;
     return MFFT_SUCCESS;
 }
 
-extern "C" int mfft_plan_set_kernel(mfft_plan* plan, int radix, int lines_per_cta) {
+extern "C" int mfft_plan_set_kernel(mfft_plan* plan, int radix, int lines_per_cta, int stages) {
     using namespace mfft;
     if (!plan) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "plan is NULL");
     if (plan->n > MFFT_MAX_SINGLE_N)
         return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "n=%lld uses the four-step path", (long long)plan->n);
-    const BatchedKernel* k = find_batched((int)plan->n, radix, lines_per_cta);
+    const BatchedKernel* k = find_batched((int)plan->n, radix, lines_per_cta, stages);
     if (!k)
-        return set_error(MFFT_ERR_KERNEL_NOT_FOUND, -1, -1, -1, "no variant n=%lld radix=%d lines_per_cta=%d",
-                         (long long)plan->n, radix, lines_per_cta);
+        return set_error(MFFT_ERR_KERNEL_NOT_FOUND, -1, -1, -1,
+                         "no variant n=%lld radix=%d lines_per_cta=%d stages=%d", (long long)plan->n, radix,
+                         lines_per_cta, stages);
     DeviceGuard g(plan->ctx->device);
     return bind_batched(plan->ctx, k, &plan->line);
 }
 
-extern "C" int mfft_list_kernels(int64_t n, int* radix, int* lines_per_cta, int cap) {
+extern "C" int mfft_list_kernels(int64_t n, int* radix, int* lines_per_cta, int* stages, int cap) {
     int cnt = 0, m = 0;
     const mfft::BatchedKernel* ks = mfft::batched_kernels(&cnt);
     for (int i = 0; i < cnt; ++i) {
@@ -158,6 +165,7 @@ extern "C" int mfft_list_kernels(int64_t n, int* radix, int* lines_per_cta, int 
         if (m < cap) {
             if (radix) radix[m] = ks[i].e;
             if (lines_per_cta) lines_per_cta[m] = ks[i].fpb;
+            if (stages) stages[m] = ks[i].stages;
         }
         ++m;
     }

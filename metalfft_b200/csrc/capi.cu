@@ -137,6 +137,13 @@ static int ctx_init(int device, mfft_ctx** out) {
         return set_error(MFFT_ERR_NO_STREAM, -1, -1, -1, "Could not create CUDA stream: %s",
                          cudaGetErrorString(e));
     }
+    e = cudaMalloc(&c->dev_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(c->dev_err, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "context error word: %s", cudaGetErrorString(e));
+    }
     *out = c;
     return MFFT_SUCCESS;
 }
@@ -176,12 +183,21 @@ extern "C" int mfft_context_destroy(mfft_ctx* ctx) {
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     for (auto& kv : ctx->twiddles) cudaFree(kv.second);
+    cudaFree(ctx->dev_err);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return MFFT_SUCCESS;
 }
 
 extern "C" int mfft_context_sm_count(const mfft_ctx* ctx) { return ctx ? ctx->sms : 0; }
+
+extern "C" int mfft_context_check(mfft_ctx* ctx) {
+    if (!ctx) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "ctx is NULL");
+    DeviceGuard g(ctx->device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_error(e, "execution");
+    return check_device_error(ctx);
+}
 
 namespace mfft {
 
@@ -285,7 +301,7 @@ int launch_c2c_device(mfft_plan* plan, const float2* in, float2* out, int64_t ba
     cudaError_t e;
     if (plan->n <= MFFT_MAX_SINGLE_N) {
         const BatchedKernel* k = plan->line.k;
-        e = (direction == MFFT_INVERSE ? k->inv : k->fwd)(in, out, batch, plan->line.tw, s);
+        e = (direction == MFFT_INVERSE ? k->inv : k->fwd)(in, out, batch, plan->line.tw, plan->ctx->dev_err, s);
         if (e != cudaSuccess) return cuda_error(e, "batched FFT launch");
         return MFFT_SUCCESS;
     }
@@ -299,6 +315,20 @@ int check_exec_args(const void* in, void* out, int64_t batch, int direction, int
     if (flags != MFFT_HOST_MEMORY && flags != MFFT_DEVICE_MEMORY)
         return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "unknown flags %d", flags);
     if (batch > 0 && (!in || !out)) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "NULL buffer");
+    return MFFT_SUCCESS;
+}
+
+// Reads and clears the context's device error word (set by a kernel whose
+// bounded wait gave up).  Synchronous.
+int check_device_error(mfft_ctx* ctx) {
+    int code = 0;
+    cudaError_t e = cudaMemcpy(&code, ctx->dev_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(e, "device error word");
+    if (code) {
+        cudaMemset(ctx->dev_err, 0, sizeof(int));
+        return set_error(MFFT_ERR_TIMEOUT, -1, -1, -1,
+                         "a device-side wait timed out (code %d); results of the call are invalid", code);
+    }
     return MFFT_SUCCESS;
 }
 
@@ -334,6 +364,7 @@ int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, s
     if (!same) cudaFreeAsync(d_out, s);
     e = cudaStreamSynchronize(s);
     if (!st && e != cudaSuccess) st = cuda_error(e, "execution");
+    if (!st) st = check_device_error(ctx);
     return st;
 }
 

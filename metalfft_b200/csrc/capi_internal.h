@@ -20,6 +20,7 @@ struct mfft_ctx {
     int l2_bytes = 0;
     bool shared = false;
     cudaStream_t stream = nullptr;
+    int* dev_err = nullptr;   // device word: first bounded-wait failure of any kernel
     std::mutex mu;
     std::map<std::pair<int, int>, float2*> twiddles;     // (n, e) -> twiddle rows
     std::map<int, const mfft::BatchedKernel*> tuned;     // n -> autotuned kernel
@@ -79,6 +80,7 @@ const BatchedKernel* tuned_batched(mfft_ctx* ctx, int n);
 int check_exec_args(const void* in, void* out, int64_t batch, int direction, int flags);
 int launch_c2c_device(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,
                       cudaStream_t s);
+int check_device_error(mfft_ctx* ctx);
 int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, size_t out_bytes,
                     const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body);
 

@@ -144,14 +144,59 @@ struct SPlan {
         for (int q = 0; q < p; ++q) s *= radix(q);
         return s;
     }
-    // offset (in float2) of pass p's twiddle rows: rows k = 0..Ns-1 of R entries
+    // float2 per twiddle row: {w1, w2, w4, w8} for radix 8/16, {w1, w2} below
+    __host__ __device__ static constexpr int twrow(int r) { return r >= 8 ? 4 : 2; }
+    // offset (in float2) of pass p's twiddle rows (k = 0 .. Ns-1)
     __host__ __device__ static constexpr int twoff(int p) {
         int o = 0;
-        for (int q = 1; q < p; ++q) o += span(q) * radix(q);
+        for (int q = 1; q < p; ++q) o += span(q) * twrow(radix(q));
         return o;
     }
     static constexpr int TWSIZE = twoff(NPASS) > 0 ? twoff(NPASS) : 2;
 };
+
+// Multiplies v[r*B] (r = 1 .. R-1) by w^r, w = e^{-2*pi*i*k/(Ns*R)}, from the
+// row {w, w^2, w^4, w^8}: the other powers are products of at most three
+// table values (w^15 = ((w * w^2) * w^4) * w^8), so every twiddle stays within
+// a few ulp while a thread reads 16 or 32 bytes per pass instead of 8*R.
+template <int R, int B>
+__device__ __forceinline__ void apply_twiddles(float2* v, const float2* __restrict__ row) {
+    const float4 q0 = __ldg(reinterpret_cast<const float4*>(row));
+    const float2 w1 = make_float2(q0.x, q0.y);
+    const float2 w2 = make_float2(q0.z, q0.w);
+    if constexpr (R == 2) {
+        v[B] = cmul(v[B], w1);
+    } else if constexpr (R == 4) {
+        v[B] = cmul(v[B], w1);
+        v[2 * B] = cmul(v[2 * B], w2);
+        v[3 * B] = cmul(v[3 * B], cmul(w1, w2));
+    } else {
+        const float4 q1 = __ldg(reinterpret_cast<const float4*>(row) + 1);
+        const float2 w4 = make_float2(q1.x, q1.y);
+        const float2 w3 = cmul(w1, w2);
+        const float2 w5 = cmul(w1, w4);
+        const float2 w6 = cmul(w2, w4);
+        const float2 w7 = cmul(w3, w4);
+        v[B] = cmul(v[B], w1);
+        v[2 * B] = cmul(v[2 * B], w2);
+        v[3 * B] = cmul(v[3 * B], w3);
+        v[4 * B] = cmul(v[4 * B], w4);
+        v[5 * B] = cmul(v[5 * B], w5);
+        v[6 * B] = cmul(v[6 * B], w6);
+        v[7 * B] = cmul(v[7 * B], w7);
+        if constexpr (R == 16) {
+            const float2 w8 = make_float2(q1.z, q1.w);
+            v[8 * B] = cmul(v[8 * B], w8);
+            v[9 * B] = cmul(v[9 * B], cmul(w1, w8));
+            v[10 * B] = cmul(v[10 * B], cmul(w2, w8));
+            v[11 * B] = cmul(v[11 * B], cmul(w3, w8));
+            v[12 * B] = cmul(v[12 * B], cmul(w4, w8));
+            v[13 * B] = cmul(v[13 * B], cmul(w5, w8));
+            v[14 * B] = cmul(v[14 * B], cmul(w6, w8));
+            v[15 * B] = cmul(v[15 * B], cmul(w7, w8));
+        }
+    }
+}
 
 // Padded shared-memory index: one spare float2 per 16 keeps the Stockham
 // write patterns (stride R*Ns) free of bank conflicts.

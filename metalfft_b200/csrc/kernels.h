@@ -7,13 +7,14 @@
 namespace mfft {
 
 typedef cudaError_t (*batched_launch_fn)(const float2* in, float2* out, long long batch,
-                                         const float2* tw, cudaStream_t s);
+                                         const float2* tw, int* dev_err, cudaStream_t s);
 
 // One instantiation of the batched in-shared-memory FFT.
 struct BatchedKernel {
     int n;         // line length
     int e;         // elements per thread (= main radix)
     int fpb;       // lines per CTA
+    int stages;    // 0: direct loads; >0: persistent, TMA bulk prefetch of `stages` groups
     int threads;   // threads per CTA
     int smem;      // dynamic shared memory per CTA (bytes)
     int tw_size;   // twiddle rows (float2) for this (n, e)
@@ -24,7 +25,7 @@ struct BatchedKernel {
 };
 
 const BatchedKernel* batched_kernels(int* count);
-const BatchedKernel* find_batched(int n, int e, int fpb);
+const BatchedKernel* find_batched(int n, int e, int fpb, int stages);
 const BatchedKernel* default_batched(int n);
 
 }  // namespace mfft

@@ -66,15 +66,8 @@ struct StockhamPass {
         if constexpr (NS > 1) {
 #pragma unroll
             for (int b = 0; b < B; ++b) {
-                const int j = t + b * T;
-                const int k = j & (NS - 1);
-                const float4* row = reinterpret_cast<const float4*>(tw + PL::twoff(P) + k * R);
-#pragma unroll
-                for (int q = 0; q < R / 2; ++q) {
-                    const float4 w = __ldg(row + q);
-                    if (q > 0) v[b + (2 * q) * B] = cmul(v[b + (2 * q) * B], make_float2(w.x, w.y));
-                    v[b + (2 * q + 1) * B] = cmul(v[b + (2 * q + 1) * B], make_float2(w.z, w.w));
-                }
+                const int k = (t + b * T) & (NS - 1);
+                apply_twiddles<R, B>(v + b, tw + PL::twoff(P) + k * PL::twrow(R));
             }
         }
 #pragma unroll
@@ -103,16 +96,17 @@ __device__ __forceinline__ void fft_regs(float2 (&v)[E], int t, const Buf& buf,
     StockhamPass<N, E, 0, WS>::run(v, t, buf, tw);
 }
 
-// Twiddle rows of pass p: tw[off + k*R + r] = e^{-2*pi*i*r*k/(Ns*R)}, in FP64
-// (sincospi) rounded once to FP32.
-__global__ void k_twiddle_rows(float2* tw, int off, int ns, int radix);
+// Twiddle rows of pass p: row k holds e^{-2*pi*i*e*k/(Ns*R)} for e = 1, 2, 4, 8
+// (first `rowlen` of them), in FP64 (sincospi) rounded once to FP32.
+__global__ void k_twiddle_rows(float2* tw, int off, int ns, int radix, int rowlen);
 
 template <int N, int E>
 inline void gen_twiddles(float2* tw, cudaStream_t s) {
     using PL = SPlan<N, E>;
     for (int p = 1; p < PL::NPASS; ++p) {
-        int cnt = PL::span(p) * PL::radix(p);
-        k_twiddle_rows<<<(cnt + 255) / 256, 256, 0, s>>>(tw, PL::twoff(p), PL::span(p), PL::radix(p));
+        int cnt = PL::span(p) * PL::twrow(PL::radix(p));
+        k_twiddle_rows<<<(cnt + 255) / 256, 256, 0, s>>>(tw, PL::twoff(p), PL::span(p), PL::radix(p),
+                                                          PL::twrow(PL::radix(p)));
     }
 }
 

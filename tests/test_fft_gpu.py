@@ -51,9 +51,13 @@ def test_every_registered_variant(M, n):
     x = O.normal_c64((5, n), seed=2000 + n)
     ref = O.truth(x)
     f = M.MetalFFT(n)
-    for radix, fpb in M.MetalFFT.variants(n):
-        f.set_kernel(radix, fpb)
-        assert O.rel_rms(f.forward_batch(x), ref) < TOL, (radix, fpb)
+    xs = O.normal_c64((1000, n), seed=2100 + n) if n <= 1024 else x  # several groups per CTA
+    refs = O.truth(xs)
+    for var in M.MetalFFT.variants(n):
+        f.set_kernel(*var)
+        assert O.rel_rms(f.forward_batch(x), ref) < TOL, var
+        assert O.rel_rms(f.inverse_batch(x), O.truth(x, inverse=True)) < TOL, var
+        assert O.rel_rms(f.forward_batch(xs), refs) < TOL, var
 
 
 @pytest.mark.parametrize("n", [64, 4096, 16384, 1 << 20])
@@ -170,10 +174,12 @@ def test_config3_full_batch_properties(M):
 
 def test_autotune_picks_a_registered_variant(M):
     import ctypes
-    r, fpb = ctypes.c_int(), ctypes.c_int()
-    st = M.lib.mfft_autotune(M.shared_context(), 1024, 4096, ctypes.byref(r), ctypes.byref(fpb))
-    assert st == 0 and (r.value, fpb.value) in M.MetalFFT.variants(1024)
+    r, fpb, stg = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    st = M.lib.mfft_autotune(M.shared_context(), 1024, 4096, ctypes.byref(r), ctypes.byref(fpb),
+                             ctypes.byref(stg))
+    assert st == 0 and (r.value, fpb.value, stg.value) in M.MetalFFT.variants(1024)
     f = M.MetalFFT(1024)
-    assert (f.kernel_info["radix"], f.kernel_info["lines_per_cta"]) == (r.value, fpb.value)
+    ki = f.kernel_info
+    assert (ki["radix"], ki["lines_per_cta"], ki["stages"]) == (r.value, fpb.value, stg.value)
     x = O.normal_c64((3, 1024), seed=77)
     assert O.rel_rms(f.forward_batch(x), O.truth(x)) < TOL
