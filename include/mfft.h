@@ -174,6 +174,20 @@ MFFT_API int mfft_exec_c2c(mfft_plan* plan, const void* in, void* out, int64_t b
 MFFT_API int mfft_exec_c2c_tc(mfft_plan* plan, const void* in, void* out, int64_t batch,
                      int direction, int variant, int flags, void* stream);
 
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (an external allocator owns the device, a real-time host reserves
+ * memory once at start-up, a plug-in host forbids allocation): the four-step
+ * FFT of `batch` lines of length n (powers of two 32768 .. 1048576, else
+ * MFFT_ERR_UNSUPPORTED_SIZE) on device pointers, enqueued on `stream`, with
+ * no allocation at all.  Its intermediate is a fixed 16 MiB device array (plus
+ * ~100 KB of tables) that every GPU loading the library holds until exit;
+ * batches go through it in chunks.  The first call on a device does a
+ * one-time set-up (launches and waits): make it before any stream capture.
+ * Calls share the array, so calls that overlap on the GPU race: serialise
+ * them. */
+MFFT_API int mfft_fourstep_noalloc(const void* in, void* out, int64_t n, int64_t batch, int direction,
+                                   void* stream);
+
 /* ---- mixed sizes in one persistent launch ------------------------------ */
 
 /* One size class: `count` transforms of length n (power of two, 64..2^20)
