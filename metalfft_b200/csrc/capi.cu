@@ -268,6 +268,7 @@ extern "C" int mfft_plan_create(mfft_ctx* ctx, int64_t n, mfft_plan** out) {
             return set_error(MFFT_ERR_KERNEL_NOT_FOUND, -1, -1, -1, "no batched kernel for n=%lld", (long long)n);
         }
         st = bind_batched(ctx, k, &p->line);
+        if (!st && n == 4096) st = tc_plan_init(p);  // tensor-core tables (mfft_exec_c2c_tc)
     } else {
         st = fourstep_plan_init(p);
     }

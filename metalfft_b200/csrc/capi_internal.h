@@ -89,6 +89,7 @@ void fourstep_plan_release(mfft_plan* plan);
 int fourstep_exec(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,
                   cudaStream_t s);
 
+int tc_plan_init(mfft_plan* plan);
 void tc_plan_release(mfft_plan* plan);
 
 }  // namespace mfft

@@ -3,15 +3,9 @@
 
 using namespace mfft;
 
-namespace mfft {
-void tc_plan_release(mfft_plan*) {}
-}  // namespace mfft
 
 #define MFFT_NOT_BUILT(name) set_error(MFFT_ERR_KERNEL_NOT_FOUND, -1, -1, -1, "%s: kernel not built", name)
 
-extern "C" int mfft_exec_c2c_tc(mfft_plan*, const void*, void*, int64_t, int, int, int, void*) {
-    return MFFT_NOT_BUILT("mfft_exec_c2c_tc");
-}
 extern "C" int mfft_multi_create(mfft_ctx*, const mfft_multi_desc*, int, mfft_multi**) {
     return MFFT_NOT_BUILT("mfft_multi_create");
 }
