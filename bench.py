@@ -10,6 +10,15 @@ headline `value` is the faster of those whose relative RMS error against an
 FP64 FFT of sampled lines is <= 3e-6.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload tc4096 | c2c4096x256 | mixed | conv]
+
+--workload selects another configuration (one JSON line each):
+  c2c4096x256  N=4096 x 256 lines U[-1,1), forward then inverse per step, over a
+               rotating pool of buffer sets larger than L2
+  mixed        sizes 64..16384 plus 2^20, seeded counts U{1..512} up to 2^26
+               points, one persistent launch per step
+  conv         overlap-add convolution of 2^24 samples with 4095 taps
+               (fftSize 8192): forward, then dx and dh, per step
 
 Under torchrun each rank transforms its own 16384 lines (weak scaling, no
 collective on the data path); rank 0 prints one JSON line.
@@ -46,6 +55,7 @@ def parse():
     p.add_argument("--batch", type=int, default=BATCH)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv"])
     return p.parse_args()
 
 
@@ -192,6 +202,118 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def timed(fn, steps, warmup, barrier, dist, uuid):
+    """Device time of `steps` calls of fn (one step each), max over ranks."""
+    import torch
+    for _ in range(max(3, warmup)):
+        fn(0)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream()
+    with ClockSampler(uuid) as clk:
+        e0.record(stream)
+        for i in range(steps):
+            fn(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), ms, clk.summary()
+
+
+def run_other(args, M, rank, world, dist, barrier, uuid):
+    """config 1 (c2c4096x256), config 2 (mixed), config 4 (conv)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+    from metalfft_b200 import workloads
+    peak, peak_src = peaks()
+    line = {"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic"}
+    if args.workload == "c2c4096x256":
+        n, b = 4096, 256
+        sets = 64  # 64 x 16 MiB = 1 GiB of rotating inputs and outputs, > L2
+        rng = np.random.default_rng(SEED + rank)
+        host = rng.uniform(-1, 1, size=(b, n, 2)).astype(np.float32).view(np.complex64)[..., 0]
+        xs = torch.from_numpy(host).cuda().unsqueeze(0).repeat(sets, 1, 1).contiguous()
+        ys = torch.empty_like(xs)
+        f = M.MetalFFT(n)
+
+        def step(i):
+            k = i % sets
+            f.exec(xs[k], ys[k], b, M.FORWARD)
+            f.exec(ys[k], xs[k], b, M.INVERSE)
+        ms_max, ms, clk = timed(step, args.steps, args.warmup, barrier, dist, uuid)
+        per_launch = ms / args.steps / 2 / 1e3
+        gbs = b * n * 16 / per_launch / 1e9
+        X = ys[0].cpu().numpy()
+        err = fp64_check(host[:8], X[:8])
+        line.update({"metric": "batched C2C FFT N=4096 x 256: transforms/s (forward + inverse)",
+                     "value": 2 * b * world * args.steps / (ms_max / 1e3), "unit": "transforms/s",
+                     "ms_per_step": ms_max / args.steps, "rel_rms": err,
+                     "config": {"workload": "C2C FFT N=4096 x 256 lines, U[-1,1) seeded, forward then inverse",
+                                "l2": "64 rotating buffer sets (1 GiB) > L2"},
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak, "peak_source": peak_src},
+                     "gpu_launches": 2 * args.steps, "clocks": clk})
+    elif args.workload == "mixed":
+        classes = workloads.mixed_size_classes()
+        mb = M.MixedBatch(classes)
+        x = torch.from_numpy(workloads.normal_c64(mb.points, SEED + rank)).cuda()
+        y = torch.empty_like(x)
+        ms_max, ms, clk = timed(lambda i: mb.exec(x, y), args.steps, args.warmup, barrier, dist, uuid)
+        assert M.lib.mfft_context_check(M.shared_context()) == 0
+        ntr = sum(c for _, c in classes)
+        gbs = mb.points * 16 / (ms / args.steps / 1e3) / 1e9
+        line.update({"metric": "mixed-size FFT batch in one persistent launch: points/s",
+                     "value": mb.points * world * args.steps / (ms_max / 1e3), "unit": "points/s",
+                     "ms_per_step": ms_max / args.steps, "transforms_per_step": ntr,
+                     "config": {"workload": "sizes 2^6..2^14 + 2^20, counts U{1..512} seeded, <= 2^26 points",
+                                "classes": classes, "points": mb.points},
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak, "peak_source": peak_src,
+                                  "note": "16 B per point algorithmic; four-step lines move 32 B"},
+                     "gpu_launches": args.steps, "clocks": clk})
+    else:
+        nx, K, fft = 1 << 24, 4095, 8192
+        xh, h, th = workloads.conv_workload(SEED + rank, nx=nx, K=K)
+        conv = M.Convolver(h, fft)
+        x = torch.from_numpy(xh).cuda()
+        t = torch.from_numpy(th).cuda()
+        y = torch.empty(nx + K - 1, device="cuda")
+        g = torch.empty_like(y)
+        dx = torch.empty_like(x)
+        dh = torch.empty(K, device="cuda")
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        P = lambda a: ctypes.c_void_p(a.data_ptr())  # noqa: E731
+
+        def step(i):
+            M._check(M.lib.mfft_conv_apply(conv._h, P(x), nx, P(y), M.DEVICE, st))
+            torch.sub(y, t, out=g)  # dL/dy for L = 0.5 ||y - t||^2
+            M._check(M.lib.mfft_conv_backward(conv._h, P(x), nx, P(g), P(dx), P(dh), M.DEVICE, st))
+        ms_max, ms, clk = timed(step, args.steps, args.warmup, barrier, dist, uuid)
+        algo = (4 * nx + 4 * (nx + K - 1)) + (4 * nx + 4 * (nx + K - 1) + 4 * nx)  # fwd + bwd bytes
+        gbs = algo / (ms / args.steps / 1e3) / 1e9
+        line.update({"metric": "fused OLA convolution forward + adjoint: samples/s",
+                     "value": nx * world * args.steps / (ms_max / 1e3), "unit": "samples/s",
+                     "ms_per_step": ms_max / args.steps,
+                     "config": {"workload": "x 2^24 N(0,1), h 4095 taps N(0,1)*exp(-t/800), fftSize 8192, "
+                                            "target N(0,1); y, then dx and dh"},
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak, "peak_source": peak_src,
+                                  "note": "algorithmic bytes: x, y read/written by forward; x, g read and dx "
+                                          "written by backward (g = y - t by one torch kernel)"},
+                     "gpu_launches": 4 * args.steps, "clocks": clk})
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -220,6 +342,18 @@ def main():
 
     import metalfft_b200 as M
 
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    if args.workload != "tc4096":
+        run_other(args, M, rank, world, dist, barrier, uuid)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
     B = args.batch
     host = make_input(B, rank)
     x = torch.from_numpy(host).cuda()
@@ -232,11 +366,6 @@ def main():
     rows = np.random.default_rng(1).choice(B, 16, replace=False)
     results = {}
     peak, peak_src = peaks()
-    uuid = None
-    try:
-        uuid = str(torch.cuda.get_device_properties(local).uuid)
-    except Exception:
-        pass
 
     for name, tc in list(variants.items()):
         try:

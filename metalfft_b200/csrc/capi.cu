@@ -336,13 +336,13 @@ int check_device_error(mfft_ctx* ctx) {
 // Host-array call: stage through one device buffer on the context stream and
 // wait, like MetalFFT's copy-in / commitAndWait / copy-out.
 int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, size_t out_bytes,
-                    const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body) {
+                    const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body, bool in_place) {
     cudaStream_t s = ctx->stream;
     void* d_in = nullptr;
     void* d_out = nullptr;
     cudaError_t e = cudaMallocAsync(&d_in, in_bytes ? in_bytes : 16, s);
     if (e != cudaSuccess) return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "Device buffer allocation failed: %s", cudaGetErrorString(e));
-    bool same = (in_bytes == out_bytes);
+    const bool same = in_place && (in_bytes == out_bytes);
     if (same) {
         d_out = d_in;
     } else {
@@ -382,7 +382,10 @@ extern "C" int mfft_exec_c2c(mfft_plan* plan, const void* in, void* out, int64_t
         return launch_c2c_device(plan, (const float2*)in, (float2*)out, batch, direction,
                                  (cudaStream_t)stream);
     size_t bytes = (size_t)batch * (size_t)plan->n * sizeof(float2);
-    return run_host_staged(plan->ctx, in, out, bytes, bytes, [&](void* di, void* dout, cudaStream_t s) {
-        return launch_c2c_device(plan, (const float2*)di, (float2*)dout, batch, direction, s);
-    });
+    return run_host_staged(
+        plan->ctx, in, out, bytes, bytes,
+        [&](void* di, void* dout, cudaStream_t s) {
+            return launch_c2c_device(plan, (const float2*)di, (float2*)dout, batch, direction, s);
+        },
+        true);
 }

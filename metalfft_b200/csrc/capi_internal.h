@@ -81,8 +81,10 @@ int check_exec_args(const void* in, void* out, int64_t batch, int direction, int
 int launch_c2c_device(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,
                       cudaStream_t s);
 int check_device_error(mfft_ctx* ctx);
+// Host-array call: copy in, run `body` on device buffers, copy out, wait.
+// in_place: the kernels may read and write one buffer (batched FFTs).
 int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, size_t out_bytes,
-                    const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body);
+                    const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body, bool in_place = false);
 
 int fourstep_plan_init(mfft_plan* plan);
 void fourstep_plan_release(mfft_plan* plan);

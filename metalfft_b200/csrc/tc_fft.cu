@@ -48,20 +48,36 @@ constexpr int TC_THREADS = 256;
 constexpr float TC_GSCALE = 16.0f;  // FP16 split: G stored as 16 * DFT-64
 constexpr int TC_LINE_EXP = 14;     // FP16 split: line scaled so |max| < 2^14
 
-// shared-memory byte offsets (dynamic)
+// shared-memory byte offsets from a 1024-byte aligned base (dynamic)
 constexpr uint32_t SM_G0 = 0;          // G hi (or bf16) : 128 x 128 halves = 32 KB
 constexpr uint32_t SM_G1 = 32768;      // G lo
 constexpr uint32_t SM_B0 = 65536;      // B hi (or bf16) : 128 x 64 halves = 16 KB
 constexpr uint32_t SM_B1 = 81920;      // B lo
-constexpr uint32_t SM_BYTES = 98304;
-constexpr uint32_t CORE_LBO = 128;     // K-group stride (bytes) in every operand
-constexpr uint32_t CORE_SBO = 2048;    // M/N-group stride (bytes) in every operand
+constexpr uint32_t SM_BYTES = 98304 + 1024;  // + alignment slack
 constexpr uint32_t TMEM_COLS = 128;    // D1: columns [0, 64), D2: [64, 128)
 
-// G (K-major), row m = 2k + b, column kk = 2n + a: byte offset in its plane
-__host__ __device__ constexpr uint32_t g_off(int m, int kk) {
-    return (m % 8) * 16 + (m / 8) * CORE_SBO + (kk / 8) * CORE_LBO + (kk % 8) * 2;
+// Operand layouts: 128-byte swizzle (1024-byte atoms of 8 rows x 128 bytes,
+// 16-byte chunk c of row r stored at chunk c ^ (r % 8)), so that the eight
+// threads of a quarter-warp storing one 128-byte row hit distinct banks.
+//  G  (A, K-major):  rows m = 2k+b (128), K = 2n+a (128) = 2 atoms of 64
+//  B1 (B, MN-major): rows = K (128), N = n2 (64 = one 128-byte row)
+//  B2 (B, K-major):  rows n = k1 (64), K = 2*n2+a (128) = 2 atoms of 64
+constexpr uint32_t G_KATOM = 16384;   // 16 row groups x 1024
+constexpr uint32_t B2_KATOM = 8192;   //  8 row groups x 1024
+constexpr uint32_t ATOM_SBO = 1024;   // stride of 8-row groups
+
+__host__ __device__ constexpr uint32_t sw128(uint32_t row, uint32_t chunk) {
+    return (row / 8) * 1024 + (row % 8) * 128 + ((chunk ^ (row % 8)) * 16);
 }
+// K-major operand with `rows` rows: element (row, kk)
+__host__ __device__ constexpr uint32_t kmaj_off(uint32_t row, uint32_t kk, uint32_t katom) {
+    return (kk / 64) * katom + sw128(row, (kk % 64) / 8) + (kk % 8) * 2;
+}
+// MN-major B1: element (nn, kk)
+__host__ __device__ constexpr uint32_t mnmaj_off(uint32_t nn, uint32_t kk) {
+    return sw128(kk, nn / 8) + (nn % 8) * 2;
+}
+__host__ __device__ constexpr uint32_t g_off(int m, int kk) { return kmaj_off(m, kk, G_KATOM); }
 
 // Tables: G planes (hi, lo with the 16x scale; bf16 unscaled) in the exact
 // shared-memory image, and T[m] = W4096^m; all from FP64 sincospi.
@@ -128,8 +144,10 @@ __device__ __forceinline__ void store_chunk(uint8_t* smem, uint32_t off, const f
     }
 }
 
-// D (+)= G * B over K = 128 (8 steps of 16): three products for the split
-template <bool SPLIT>
+// D (+)= G * B over K = 128 (8 steps of 16): three products for the split.
+// K step j: K-major operands advance (j/4) atoms plus (j%4)*32 bytes inside
+// the 128-byte row; the MN-major B1 advances two 8-row groups.
+template <bool SPLIT, bool B_MN>
 __device__ __forceinline__ void issue_product(uint32_t d_tmem, uint32_t smem_base, uint32_t idesc) {
     constexpr int NPROD = SPLIT ? 3 : 1;
 #pragma unroll
@@ -138,8 +156,10 @@ __device__ __forceinline__ void issue_product(uint32_t d_tmem, uint32_t smem_bas
         const uint32_t bb = smem_base + (p == 1 ? SM_B1 : SM_B0);
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            const uint64_t ad = tc::smem_desc(ga + 256u * j, CORE_LBO, CORE_SBO);
-            const uint64_t bd = tc::smem_desc(bb + 256u * j, CORE_LBO, CORE_SBO);
+            const uint64_t ad = tc::smem_desc(ga + (j / 4) * G_KATOM + (j % 4) * 32, 16, ATOM_SBO, tc::LAYOUT_SW128);
+            const uint64_t bd =
+                B_MN ? tc::smem_desc(bb + 2 * j * ATOM_SBO, 16384, ATOM_SBO, tc::LAYOUT_SW128)
+                     : tc::smem_desc(bb + (j / 4) * B2_KATOM + (j % 4) * 32, 16, ATOM_SBO, tc::LAYOUT_SW128);
             tc::mma_f16_ss(d_tmem, ad, bd, idesc, (p > 0 || j > 0) ? 1u : 0u);
         }
     }
@@ -149,7 +169,7 @@ template <bool SPLIT, bool INV>
 __global__ void __launch_bounds__(TC_THREADS, 2)
     k_fft4096_tc(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
                  const uint4* __restrict__ gimg, const float2* __restrict__ tw, int* dev_err) {
-    extern __shared__ __align__(1024) uint8_t smem[];
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base_sh;
     __shared__ float red1[TC_THREADS / 32], red2[TC_THREADS / 32];
@@ -157,6 +177,8 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
+    // swizzle atoms need 1024-byte alignment
+    uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const uint32_t sbase = smem_u32(smem);
     constexpr uint32_t FMT = SPLIT ? 0u : 1u;
     constexpr uint32_t IDESC1 = tc::idesc_f16(FMT, 1u, 128, 64);  // B MN-major
@@ -224,11 +246,9 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
                 re[2 * j + 1] = v.z * s1;
                 im[2 * j + 1] = v.w * s1;
             }
-            // MN-major: (nn, kk) at (nn%8)*2 + (nn/8)*SBO + (kk%8)*16 + (kk/8)*LBO
-            const int kr = 2 * n1;
-            const uint32_t off_re = c * CORE_SBO + (kr / 8) * CORE_LBO + (kr % 8) * 16;
-            store_chunk<SPLIT>(smem, off_re, re);
-            store_chunk<SPLIT>(smem, off_re + 16, im);  // kk = 2*n1 + 1
+            // MN-major rows kk = 2*n1 (re) and 2*n1 + 1 (im), chunk c of n2
+            store_chunk<SPLIT>(smem, mnmaj_off(8 * c, 2 * n1), re);
+            store_chunk<SPLIT>(smem, mnmaj_off(8 * c, 2 * n1 + 1), im);
         }
         // prefetch the next line: in flight during the tensor-core work
         if (f + gridDim.x < batch) load_line(f + gridDim.x);
@@ -239,7 +259,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
         // ---- stage 1 on the tensor cores ----
         if (tid == 0) {
             tc::fence_after_sync();
-            issue_product<SPLIT>(d1, sbase, IDESC1);
+            issue_product<SPLIT, true>(d1, sbase, IDESC1);
             tc::mma_commit(&mbar);
             if (!mbar_wait(&mbar, phase)) abort_sh = 1;
         }
@@ -272,9 +292,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
         tc::fence_before_sync();
         const float s2 = SPLIT ? line_scale(block_max(mx2, red2, tid)) : 1.f;
         {
-            // K-major: (nn = k1, kk = 2*n2 + a) at (nn%8)*16 + (nn/8)*SBO + (kk/8)*LBO + (kk%8)*2
-            const uint32_t rowoff = (kk_ % 8) * 16 + (kk_ / 8) * CORE_SBO;
-            const int kg0 = n2_0 / 4;
+            // K-major row nn = k1, K = 2*n2 + a: 4 chunks of 8 (4 complex values)
 #pragma unroll
             for (int qq = 0; qq < 4; ++qq) {
                 float x[8];
@@ -283,7 +301,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
                     x[2 * j] = z[4 * qq + j].x * s2;
                     x[2 * j + 1] = z[4 * qq + j].y * s2;
                 }
-                store_chunk<SPLIT>(smem, rowoff + (kg0 + qq) * CORE_LBO, x);
+                store_chunk<SPLIT>(smem, kmaj_off(kk_, 2 * (n2_0 + 4 * qq), B2_KATOM), x);
             }
         }
         fence_proxy_async_smem();
@@ -293,7 +311,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
         // ---- stage 2 on the tensor cores ----
         if (tid == 0) {
             tc::fence_after_sync();
-            issue_product<SPLIT>(d2, sbase, IDESC2);
+            issue_product<SPLIT, false>(d2, sbase, IDESC2);
             tc::mma_commit(&mbar);
             if (!mbar_wait(&mbar, phase)) abort_sh = 1;
         }
@@ -430,7 +448,10 @@ extern "C" int mfft_exec_c2c_tc(mfft_plan* plan, const void* in, void* out, int6
     if (flags == MFFT_DEVICE_MEMORY)
         return tc_launch(plan, (const float2*)in, (float2*)out, batch, direction, variant, (cudaStream_t)stream);
     size_t bytes = (size_t)batch * TC_N * sizeof(float2);
-    return run_host_staged(plan->ctx, in, out, bytes, bytes, [&](void* di, void* dout, cudaStream_t s) {
-        return tc_launch(plan, (const float2*)di, (float2*)dout, batch, direction, variant, s);
-    });
+    return run_host_staged(
+        plan->ctx, in, out, bytes, bytes,
+        [&](void* di, void* dout, cudaStream_t s) {
+            return tc_launch(plan, (const float2*)di, (float2*)dout, batch, direction, variant, s);
+        },
+        true);
 }

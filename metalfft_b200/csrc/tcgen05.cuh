@@ -33,17 +33,28 @@ __device__ __forceinline__ void fence_after_sync() {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-// ---- shared-memory matrix descriptor, SWIZZLE_NONE canonical layout ---------
-// K-major:  element (row r, k) at (r%8)*16 + (r/8)*SBO + (k/8)*LBO + (k%8)*2 bytes
-// MN-major: element (mn, k)    at (mn%8)*2 + (mn/8)*SBO + (k%8)*16 + (k/8)*LBO bytes
-// (8-row x 16-byte core matrices; LBO steps along K, SBO along M/N).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+// ---- shared-memory matrix descriptor --------------------------------------
+// layout 0 = SWIZZLE_NONE: 8-row x 16-byte core matrices,
+//   K-major:  element (row r, k) at (r%8)*16 + (r/8)*SBO + (k/8)*LBO + (k%8)*2
+//   MN-major: element (mn, k)    at (mn%8)*2 + (mn/8)*SBO + (k%8)*16 + (k/8)*LBO
+// layout 2 = SWIZZLE_128B: 1024-byte atoms of 8 rows x 128 bytes in which the
+//   16-byte chunk index (address bits 4-6) is XORed with the row index
+//   (address bits 7-9); atoms must be 1024-byte aligned.
+//   K-major:  row = M/N index (atoms of 8 rows at SBO), 64 K elements per row
+//             (LBO = 16, unused); a K step inside the atom advances the start
+//             address by its unswizzled byte offset.
+//   MN-major: row = K index (atoms of 8 K rows at SBO), 64 M/N elements per
+//             row (further 64-element groups at LBO).
+constexpr uint32_t LAYOUT_NONE = 0, LAYOUT_SW128 = 2;
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo,
+                                             uint32_t layout = LAYOUT_NONE) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);
     d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
     d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
     d |= (uint64_t)1 << 46;  // descriptor version for sm_100
-    // base offset 0, LBO mode 0, layout type 0 (SWIZZLE_NONE)
+    d |= (uint64_t)(layout & 7) << 61;
+    // base offset 0 (atoms 1024-byte aligned), LBO mode 0
     return d;
 }
 

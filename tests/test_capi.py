@@ -57,3 +57,17 @@ def test_no_device_is_reported_not_faked():
     buf = ctypes.create_string_buffer(256)
     assert lib.mfft_last_error(buf, 256) == 1
     assert b"No CUDA device" in buf.value
+
+
+def test_window_coefficients_match_oracle():
+    import numpy as np
+
+    from metalfft_b200 import _lib
+    from oracle import oracle as O
+    lib = _lib.load()
+    for kind in range(6):
+        for n in [8, 64, 1024]:
+            w = np.empty(n, np.float32)
+            assert lib.mfft_window(kind, n, 6.0, w.ctypes.data) == 0
+            assert np.max(np.abs(w - O.window(kind, n, 6.0))) < 1e-6
+    assert lib.mfft_window(9, 8, 0.0, w.ctypes.data) == 10
