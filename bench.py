@@ -10,7 +10,7 @@ headline `value` is the faster of those whose relative RMS error against an
 FP64 FFT of sampled lines is <= 3e-6.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tc4096 | c2c4096x256 | mixed | conv]
+                    [--workload tc4096 | c2c4096x256 | mixed | conv | sar]
 
 --workload selects another configuration (one JSON line each):
   c2c4096x256  N=4096 x 256 lines U[-1,1), forward then inverse per step, over a
@@ -19,6 +19,9 @@ FP64 FFT of sampled lines is <= 3e-6.
                points, one persistent launch per step
   conv         overlap-add convolution of 2^24 samples with 4095 taps
                (fftSize 8192): forward, then dx and dh, per step
+  sar          FP16 SAR chain 4096 pulses x 8192 range (64 targets, 10 dB):
+               range matched filter, corner turn, azimuth FFT and the phase
+               adjoint of sum |I|^4, one CUDA graph per step
 
 Under torchrun each rank transforms its own 16384 lines (weak scaling, no
 collective on the data path); rank 0 prints one JSON line.
@@ -55,7 +58,7 @@ def parse():
     p.add_argument("--batch", type=int, default=BATCH)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv"])
+    p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv", "sar"])
     return p.parse_args()
 
 
@@ -280,6 +283,29 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
                                   "frac": gbs / peak, "peak_source": peak_src,
                                   "note": "16 B per point algorithmic; four-step lines move 32 B"},
                      "gpu_launches": args.steps, "clocks": clk})
+    elif args.workload == "sar":
+        prm = M.SARParameters.default(4096, 8192, 1024, 512.0)
+        sar = M.SARPipeline(prm)
+        raw = sar.simulate(workloads.sar_targets(prm, 64, seed=SEED + rank), 10.0, SEED + rank)
+        h, sc = sar.quantize(raw)
+        del raw
+        phi = torch.from_numpy(workloads.sar_phase(prm.pulses, seed=SEED + rank)).cuda()
+        out = sar.step(h, sc, phi)
+        ms_max, ms, clk = timed(lambda i: sar.step(h, sc, phi, out), args.steps, args.warmup, barrier, dist, uuid)
+        ns = prm.pulses * prm.range_n
+        algo = ns * 16  # pass A: FP16 in + out, pass B: FP16 in + out
+        gbs = algo / (ms / args.steps / 1e3) / 1e9
+        line.update({"metric": "FP16 SAR range-Doppler + phase adjoint: complex samples/s",
+                     "value": ns * world * args.steps / (ms_max / 1e3), "unit": "samples/s",
+                     "ms_per_step": ms_max / args.steps, "dtype": "fp16 storage, fp32 compute",
+                     "loss": float(out[3].item()),
+                     "config": {"workload": "4096 pulses x 8192 range, chirp 1024 samples TBP 512, 64 seeded "
+                                            "targets, 10 dB SNR, phase N(0,0.3); image + dL/dphi of sum |I|^4",
+                                "graph": "one CUDA graph per step (range pass, azimuth+adjoint pass, reduce)"},
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak, "peak_source": peak_src,
+                                  "note": "16 B per complex sample: two passes of FP16 in + out"},
+                     "gpu_launches": 3 * args.steps, "clocks": clk})
     else:
         nx, K, fft = 1 << 24, 4095, 8192
         xh, h, th = workloads.conv_workload(SEED + rank, nx=nx, K=K)

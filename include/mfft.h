@@ -254,6 +254,77 @@ MFFT_API int mfft_analyzer_destroy(mfft_analyzer* a);
 MFFT_API int mfft_analyzer_analyze(mfft_analyzer* a, const float* samples, int64_t count,
                           int64_t offset, void* spectrum, int flags, void* stream);
 
+/* ---- SAR range-Doppler chain (src/radar/, src/fft_sar_fused*.metal) ----- */
+
+/* SARParameters (src/radar/sar_simulator.swift:22-67) with the chirp given by
+ * its sample count: Tp = chirp_samples / sample_rate, Kr = bandwidth / Tp,
+ * lambda = c / carrier, fast time t_r = 2*center_range/c - (range_n/2)/fs +
+ * r/fs, slow time eta_p = (p - pulses/2)/prf. */
+typedef struct mfft_sar_params {
+    int64_t pulses;        /* azimuth lines Na (64 .. 4096, power of two)  */
+    int64_t range_n;       /* range samples Nr (512 .. 16384, power of two) */
+    int64_t chirp_samples; /* Tp * fs                                       */
+    double bandwidth;      /* B, Hz                                         */
+    double sample_rate;    /* fs, Hz                                        */
+    double prf;            /* Hz                                            */
+    double velocity;       /* m/s                                           */
+    double carrier;        /* Hz                                            */
+    double center_range;   /* m                                             */
+} mfft_sar_params;
+
+/* PointTarget (sar_simulator.swift:69-78) plus a reflection phase. */
+typedef struct mfft_sar_target {
+    double range_m;   /* slant range at closest approach */
+    double azimuth_m; /* along-track position            */
+    double amplitude;
+    double phase;     /* rad */
+} mfft_sar_target;
+
+typedef struct mfft_sar mfft_sar;
+
+/* The reference's parameters (SARParameters.init: B = 100 MHz, PRF 1 kHz,
+ * v = 100 m/s, X band 10 GHz, 20 km scene centre) with the chirp set by its
+ * sample count and time-bandwidth product: fs = chirp_samples * B / tbp. */
+MFFT_API int mfft_sar_default_params(int64_t pulses, int64_t range_n, int64_t chirp_samples, double tbp,
+                                     mfft_sar_params* out);
+/* generateChirpReference (sar_simulator.swift:209-224): the chirp centred
+ * circularly at sample 0, range_n complex64 values (host memory). */
+MFFT_API int mfft_sar_chirp_reference(const mfft_sar_params* p, void* chirp);
+/* SARSimulator.simulate (sar_simulator.swift:93-205) on the device: echoes of
+ * the targets (chirp exp(j*pi*Kr*dt^2), two-way phase exp(-j*4*pi*R/lambda),
+ * reflection phase) plus complex Gaussian noise at snr_db relative to the mean
+ * power of the non-zero samples (addNoise, :161-204) drawn from a
+ * counter-based generator of `seed`.  raw: pulses x range_n complex64,
+ * device memory, pulse-major. */
+MFFT_API int mfft_sar_simulate(mfft_ctx* ctx, const mfft_sar_params* p, const mfft_sar_target* targets,
+                               int ntargets, double snr_db, uint64_t seed, void* raw, void* stream);
+/* FP16 storage with one power-of-two scale per pulse: raw_h[p][r] * scale[p]
+ * ~= raw[p][r].  Device memory. */
+MFFT_API int mfft_sar_quantize(mfft_ctx* ctx, int64_t pulses, int64_t range_n, const void* raw,
+                               void* raw_h, float* pulse_scale, void* stream);
+
+/* Range matched filter H = conj(FFT(chirp_ref)) (rda_fused_pipeline.swift:
+ * 189-196) and the work buffers of one pulses x range_n geometry. */
+MFFT_API int mfft_sar_create(mfft_ctx* ctx, const mfft_sar_params* p, const void* chirp_ref, mfft_sar** out);
+MFFT_API int mfft_sar_destroy(mfft_sar* sar);
+/* Forward image I[k][r] = sum_p W_Na^{pk} u_p[r], u_p = range-compressed pulse
+ * p times exp(j*phase[p]): fused range compression (fused_range_compression,
+ * src/fft_sar_fused.metal:246-293) then the azimuth FFT with the corner turn
+ * folded into its tile loads (azimuthFFT, rda_fused_pipeline.swift:224-242).
+ * Input FP16 pulse-major with pulse scales; output FP16 azimuth-major
+ * (image[k*range_n + r]) with one scale per range column.  Device memory. */
+MFFT_API int mfft_sar_forward(mfft_sar* sar, const void* raw_h, const float* pulse_scale, const float* phase,
+                              void* image_h, float* image_scale, void* stream);
+/* Adjoint of L = sum |I|^4 with respect to phase (no reference counterpart):
+ * dphi[p] = -sum_r Im(u_p[r] conj(B[p][r])), B = sum_k 4|I|^2 I W^{-pk};
+ * the loss goes to *loss (device double).  Recomputes the range pass. */
+MFFT_API int mfft_sar_backward_phase(mfft_sar* sar, const void* raw_h, const float* pulse_scale,
+                                     const float* phase, float* dphi, double* loss, void* stream);
+/* Forward + backward as one CUDA graph, captured on the first call for these
+ * pointers and replayed on later calls with the same pointers. */
+MFFT_API int mfft_sar_step_graph(mfft_sar* sar, const void* raw_h, const float* pulse_scale, const float* phase,
+                                 void* image_h, float* image_scale, float* dphi, double* loss, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,7 +31,8 @@ from . import _lib
 
 __all__ = [
     "FFTError", "MetalFFT", "MultiChannelFFT", "Convolver", "FusedConvolver", "Correlator",
-    "FFTAnalyzer", "AnalysisResult", "WindowType", "MixedBatch", "lib", "shared_context",
+    "FFTAnalyzer", "AnalysisResult", "WindowType", "MixedBatch", "SARParameters", "SARTarget",
+    "SARPipeline", "lib", "shared_context",
 ]
 
 lib = _lib.load()
@@ -260,3 +261,4 @@ class MultiChannelFFT:
 
 from ._dsp import (AnalysisResult, Convolver, Correlator, FFTAnalyzer, FusedConvolver,  # noqa: E402
                    MixedBatch, WindowType)
+from ._sar import SARParameters, SARPipeline, SARTarget  # noqa: E402

@@ -60,6 +60,17 @@ SIGNATURES = [
     ("mfft_analyzer_destroy", c_int, [c_void_p]),
     ("mfft_analyzer_analyze", c_int,
      [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int, c_void_p]),
+    ("mfft_sar_default_params", c_int, [c_int64, c_int64, c_int64, c_double, c_void_p]),
+    ("mfft_sar_chirp_reference", c_int, [c_void_p, c_void_p]),
+    ("mfft_sar_simulate", c_int, [c_void_p, c_void_p, c_void_p, c_int, c_double, ctypes.c_uint64, c_void_p,
+                                  c_void_p]),
+    ("mfft_sar_quantize", c_int, [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("mfft_sar_create", c_int, [c_void_p, c_void_p, c_void_p, P(c_void_p)]),
+    ("mfft_sar_destroy", c_int, [c_void_p]),
+    ("mfft_sar_forward", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("mfft_sar_backward_phase", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("mfft_sar_step_graph", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_void_p]),
 ]
 
 _lib = None

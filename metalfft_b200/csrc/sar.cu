@@ -1,0 +1,644 @@
+// sar.cu -- SAR range-Doppler chain with FP16 storage and its phase adjoint.
+//
+// Reference: RDAFusedPipeline (src/radar/rda_fused_pipeline.swift:131-242):
+// fused range compression per pulse (FFT -> * conj(FFT(chirp)) -> IFFT,
+// src/fft_sar_fused.metal:246-293, N_FFT = 4096 hard-coded), then the azimuth
+// FFT as transpose_2d -> batched FFT -> transpose_2d, each step its own
+// command buffer with FP32 device data; FP16 only in threadgroup memory
+// (fft_sar_fused_fp16.metal:10-33).  The simulator is SARSimulator
+// (src/radar/sar_simulator.swift:79-245).
+//
+// Here (two passes over HBM, FP16 storage with power-of-two block scales):
+//   pass A  k_sar_range   one pulse per CTA: FP16 samples * pulse scale *
+//                         e^{j phi_p} -> FFT -> * H -> IFFT -> FP16 with a new
+//                         per-pulse scale, pulse-major (the scale of each
+//                         pulse travels with it through the corner turn)
+//   pass B  k_sar_azimuth a tile of C range columns x all pulses per CTA: the
+//                         corner turn is the tile load itself (each row of the
+//                         tile is C consecutive range bins); FFT along azimuth
+//                         -> FP16 image (azimuth-major, one scale per range
+//                         column) and/or the adjoint of L = sum |I|^4 with
+//                         respect to phi: G = 4|I|^2 I, B = sum_k G W^{-pk}
+//                         (one more FFT on the registers), per-tile partials
+//                         of dphi_p = -sum_r Im(u_p[r] conj(B[p][r]))
+//   reduce  k_sar_reduce  partials summed over tiles in a fixed order (FP64)
+#include <cuda_fp16.h>
+
+#include <vector>
+
+#include "capi_internal.h"
+#include "stockham.cuh"
+
+namespace mfft {
+namespace {
+
+constexpr double C_LIGHT = 299792458.0;
+constexpr double PI_D = 3.14159265358979323846;
+constexpr int SAR_E = 16;
+
+struct SarGeom {
+    long long na, nr;
+    double fs, prf, v, tp, kr, lambda, tau0;
+};
+
+SarGeom make_geom(const mfft_sar_params& p) {
+    SarGeom g;
+    g.na = p.pulses;
+    g.nr = p.range_n;
+    g.fs = p.sample_rate;
+    g.prf = p.prf;
+    g.v = p.velocity;
+    g.tp = (double)p.chirp_samples / p.sample_rate;
+    g.kr = p.bandwidth / g.tp;
+    g.lambda = C_LIGHT / p.carrier;
+    g.tau0 = 2.0 * p.center_range / C_LIGHT - (double)(p.range_n / 2) / p.sample_rate;
+    return g;
+}
+
+// counter-based generator (splitmix64 finaliser), identical on host and device
+__host__ __device__ inline uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ inline double unit_open(uint64_t seed, uint64_t idx) {
+    return ((double)(mix64(seed ^ mix64(idx)) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+__global__ void k_sar_signal(float2* __restrict__ raw, SarGeom g, const mfft_sar_target* __restrict__ tg, int nt) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= g.na * g.nr) return;
+    const long long p = idx / g.nr, r = idx % g.nr;
+    const double eta = (double)(p - g.na / 2) / g.prf;
+    const double tr = g.tau0 + (double)r / g.fs;
+    double re = 0.0, im = 0.0;
+    for (int i = 0; i < nt; ++i) {
+        const double dx = g.v * eta - tg[i].azimuth_m;
+        const double R = sqrt(tg[i].range_m * tg[i].range_m + dx * dx);
+        const double dt = tr - 2.0 * R / C_LIGHT;
+        if (fabs(dt) <= g.tp / 2.0) {
+            const double ph = PI_D * g.kr * dt * dt - 4.0 * PI_D * R / g.lambda + tg[i].phase;
+            double s, c;
+            sincos(ph, &s, &c);
+            re += tg[i].amplitude * c;
+            im += tg[i].amplitude * s;
+        }
+    }
+    raw[idx] = make_float2((float)re, (float)im);
+}
+
+// per-block partial sums of |s|^2 over non-zero samples and their count
+__global__ void k_sar_power(const float2* __restrict__ raw, long long n, double* __restrict__ part) {
+    __shared__ double ss[256], sc[256];
+    double s = 0.0, c = 0.0;
+    for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+        const float2 v = raw[i];
+        const double m = (double)v.x * v.x + (double)v.y * v.y;
+        if (m > 0.0) {
+            s += m;
+            c += 1.0;
+        }
+    }
+    ss[threadIdx.x] = s;
+    sc[threadIdx.x] = c;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            ss[threadIdx.x] += ss[threadIdx.x + o];
+            sc[threadIdx.x] += sc[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = ss[0];
+        part[2 * blockIdx.x + 1] = sc[0];
+    }
+}
+
+// complex Gaussian noise: per-sample Box-Muller on two counter-based uniforms,
+// std per component sqrt(P / (2 * 10^(snr/10))), P from the partial sums
+__global__ void k_sar_noise(float2* __restrict__ raw, long long n, const double* __restrict__ part, int nparts,
+                            double snr_db, uint64_t seed) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    double s = 0.0, c = 0.0;
+    for (int i = 0; i < nparts; ++i) {
+        s += part[2 * i];
+        c += part[2 * i + 1];
+    }
+    if (c <= 0.0) return;
+    const double sigma = sqrt((s / c) / pow(10.0, snr_db / 10.0) / 2.0);
+    const double u1 = unit_open(seed, 2 * (uint64_t)idx), u2 = unit_open(seed, 2 * (uint64_t)idx + 1);
+    const double rr = sigma * sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    const float2 v = raw[idx];
+    raw[idx] = make_float2((float)(v.x + rr * cs), (float)(v.y + rr * sn));
+}
+
+// power-of-two block scale s with max|v| / s < 2^15 (1 for an all-zero block)
+__device__ __forceinline__ float block_scale(float mx) {
+    if (!(mx > 0.f)) return 1.f;
+    int e;
+    frexpf(mx, &e);
+    return ldexpf(1.f, e - 15);
+}
+
+__device__ __forceinline__ float cta_max(float v, float* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[w] = v;
+    __syncthreads();
+    float m = red[0];
+    for (int i = 1; i < nw; ++i) m = fmaxf(m, red[i]);
+    return m;
+}
+
+__global__ void k_sar_quantize(const float2* __restrict__ raw, long long nr, __half2* __restrict__ out,
+                               float* __restrict__ scale) {
+    __shared__ float red[32];
+    const long long p = blockIdx.x;
+    const float2* row = raw + p * nr;
+    float mx = 0.f;
+    for (long long i = threadIdx.x; i < nr; i += blockDim.x) {
+        const float2 v = row[i];
+        mx = fmaxf(mx, fmaxf(fabsf(v.x), fabsf(v.y)));
+    }
+    const float s = block_scale(cta_max(mx, red));
+    const float inv = 1.f / s;
+    for (long long i = threadIdx.x; i < nr; i += blockDim.x) {
+        const float2 v = row[i];
+        out[p * nr + i] = __floats2half2_rn(v.x * inv, v.y * inv);
+    }
+    if (threadIdx.x == 0) scale[p] = s;
+}
+
+// pass A: range compression of one pulse per CTA
+template <int NR>
+__global__ void __launch_bounds__(NR / SAR_E) k_sar_range(const __half2* __restrict__ raw, const float* __restrict__ pscale,
+                                                           const float* __restrict__ phase, const float2* __restrict__ H,
+                                                           const float2* __restrict__ tw, __half2* __restrict__ rc,
+                                                           float* __restrict__ rc_scale) {
+    constexpr int T = NR / SAR_E;
+    extern __shared__ __align__(16) float2 smem[];
+    __shared__ float red[32];
+    const long long p = blockIdx.x;
+    const int t = threadIdx.x;
+    float sp, cp;
+    sincosf(phase[p], &sp, &cp);
+    const float sc = pscale[p];
+    const float2 rot = make_float2(cp * sc, sp * sc);
+    float2 v[SAR_E];
+#pragma unroll
+    for (int m = 0; m < SAR_E; ++m) v[m] = cmul(__half22float2(raw[p * NR + t + m * T]), rot);
+    fft_regs<NR, SAR_E, (T <= 32)>(v, t, PadLine{smem}, tw);
+#pragma unroll
+    for (int m = 0; m < SAR_E; ++m) v[m] = cconj(cmul(v[m], __ldg(H + t + m * T)));
+    fft_regs<NR, SAR_E, (T <= 32)>(v, t, PadLine{smem}, tw);
+    float mx = 0.f;
+    const float inv_n = 1.f / (float)NR;
+#pragma unroll
+    for (int m = 0; m < SAR_E; ++m) {
+        v[m] = make_float2(v[m].x * inv_n, -v[m].y * inv_n);
+        mx = fmaxf(mx, fmaxf(fabsf(v[m].x), fabsf(v[m].y)));
+    }
+    const float s = block_scale(cta_max(mx, red));
+    const float inv = 1.f / s;
+#pragma unroll
+    for (int m = 0; m < SAR_E; ++m) rc[p * NR + t + m * T] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
+    if (t == 0) rc_scale[p] = s;
+}
+
+template <int NA>
+struct AzGeom {
+    static constexpr int T = NA / SAR_E;
+    static constexpr int C = (16384 / NA) < 16 ? (16384 / NA) : 16;  // range columns per CTA
+    static constexpr int THREADS = T * C;
+};
+
+// pass B: azimuth FFT of C range columns; IMAGE: write the FP16 image;
+// GRAD: per-tile partials of dL/dphi and of L = sum |I|^4
+template <int NA, bool IMAGE, bool GRAD>
+__global__ void __launch_bounds__(AzGeom<NA>::THREADS)
+    k_sar_azimuth(const __half2* __restrict__ rc, const float* __restrict__ rc_scale, long long nr,
+                  const float2* __restrict__ tw, __half2* __restrict__ image, float* __restrict__ image_scale,
+                  float* __restrict__ dphi_part, double* __restrict__ loss_part) {
+    constexpr int T = AzGeom<NA>::T, C = AzGeom<NA>::C;
+    extern __shared__ __align__(16) float2 smem[];
+    __shared__ float red[32][C];
+    __shared__ double lred[32];
+    const long long tile = blockIdx.x;
+    const int c = threadIdx.x % C, t = threadIdx.x / C;
+    const long long col = tile * C + c;
+    float2 v[SAR_E];
+#pragma unroll
+    for (int m = 0; m < SAR_E; ++m) {
+        const int p = t + m * T;
+        const float2 u = __half22float2(rc[(long long)p * nr + col]);
+        const float s = __ldg(rc_scale + p);
+        v[m] = make_float2(u.x * s, u.y * s);
+    }
+    fft_regs<NA, SAR_E, false>(v, t, ColLine<C>{smem, c}, tw);  // v[m] = I[k = t + m*T][col]
+    if constexpr (IMAGE) {
+        float mx = 0.f;
+#pragma unroll
+        for (int m = 0; m < SAR_E; ++m) mx = fmaxf(mx, fmaxf(fabsf(v[m].x), fabsf(v[m].y)));
+        // max over the T threads of column c: lanes differing in t share a warp
+        // when C < 32 (t varies across lane bits above log2 C)
+#pragma unroll
+        for (int o = 16; o >= C; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        const int w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) < C) red[w][c] = mx;
+        __syncthreads();
+        float cm = 0.f;
+        for (int i = 0; i < (AzGeom<NA>::THREADS + 31) / 32; ++i) cm = fmaxf(cm, red[i][c]);
+        const float s = block_scale(cm);
+        const float inv = 1.f / s;
+#pragma unroll
+        for (int m = 0; m < SAR_E; ++m)
+            image[(long long)(t + m * T) * nr + col] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
+        if (t == 0) image_scale[col] = s;
+    }
+    if constexpr (GRAD) {
+        double lsum = 0.0;
+#pragma unroll
+        for (int m = 0; m < SAR_E; ++m) {
+            const float a2 = v[m].x * v[m].x + v[m].y * v[m].y;
+            lsum += (double)a2 * (double)a2;
+            v[m] = make_float2(4.f * a2 * v[m].x, -4.f * a2 * v[m].y);  // conj(G)
+        }
+        fft_regs<NA, SAR_E, false>(v, t, ColLine<C>{smem, c}, tw);  // conj(B[p]), p = t + m*T
+        float d[SAR_E];
+#pragma unroll
+        for (int m = 0; m < SAR_E; ++m) {
+            const int p = t + m * T;
+            const float2 u0 = __half22float2(rc[(long long)p * nr + col]);
+            const float s = __ldg(rc_scale + p);
+            const float2 u = make_float2(u0.x * s, u0.y * s);
+            // -Im(u conj(B)) with v = conj(B): -Im(u v)
+            d[m] = -(u.x * v[m].y + u.y * v[m].x);
+        }
+        // sum over the C columns of the tile: c is the low part of the lane id
+#pragma unroll
+        for (int m = 0; m < SAR_E; ++m)
+#pragma unroll
+            for (int o = 1; o < C && o < 32; o <<= 1) d[m] += __shfl_xor_sync(0xffffffffu, d[m], o);
+        if (c == 0) {
+#pragma unroll
+            for (int m = 0; m < SAR_E; ++m) dphi_part[tile * NA + t + m * T] = d[m];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        if ((threadIdx.x & 31) == 0) lred[threadIdx.x >> 5] = lsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int i = 0; i < (AzGeom<NA>::THREADS + 31) / 32; ++i) tot += lred[i];
+            loss_part[tile] = tot;
+        }
+    }
+}
+
+// dphi[p] = sum over tiles (fixed order); loss = sum of the tile losses
+__global__ void k_sar_reduce(const float* __restrict__ part, long long tiles, long long na, float* __restrict__ dphi,
+                             const double* __restrict__ loss_part, double* __restrict__ loss) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < na) {
+        double s = 0.0;
+        for (long long i = 0; i < tiles; ++i) s += part[i * na + p];
+        dphi[p] = (float)s;
+    }
+    if (p == 0 && loss) {
+        double s = 0.0;
+        for (long long i = 0; i < tiles; ++i) s += loss_part[i];
+        *loss = s;
+    }
+}
+
+typedef void (*range_fn)(int grid, cudaStream_t, const __half2*, const float*, const float*, const float2*,
+                         const float2*, __half2*, float*);
+typedef void (*az_fn)(int grid, cudaStream_t, const __half2*, const float*, long long, const float2*, __half2*, float*,
+                      float*, double*);
+
+template <int NR>
+void l_range(int grid, cudaStream_t s, const __half2* raw, const float* ps, const float* ph, const float2* H,
+             const float2* tw, __half2* rc, float* rcs) {
+    k_sar_range<NR><<<grid, NR / SAR_E, spad_size(NR) * 8, s>>>(raw, ps, ph, H, tw, rc, rcs);
+}
+template <int NA, bool IMAGE, bool GRAD>
+void l_az(int grid, cudaStream_t s, const __half2* rc, const float* rcs, long long nr, const float2* tw, __half2* img,
+          float* imgs, float* dp, double* lp) {
+    k_sar_azimuth<NA, IMAGE, GRAD><<<grid, AzGeom<NA>::THREADS, NA * AzGeom<NA>::C * 8, s>>>(rc, rcs, nr, tw, img, imgs,
+                                                                                            dp, lp);
+}
+template <int NR>
+cudaError_t prep_range() {
+    return cudaFuncSetAttribute(k_sar_range<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, spad_size(NR) * 8);
+}
+template <int NA>
+cudaError_t prep_az() {
+    const int sm = NA * AzGeom<NA>::C * 8;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_sar_azimuth<NA, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    if ((e = cudaFuncSetAttribute(k_sar_azimuth<NA, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    return cudaFuncSetAttribute(k_sar_azimuth<NA, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+struct RangeK {
+    int n;
+    range_fn f;
+    cudaError_t (*prep)();
+};
+struct AzK {
+    int n, cols;
+    az_fn fwd, bwd, both;
+    cudaError_t (*prep)();
+};
+const RangeK g_range[] = {{512, &l_range<512>, &prep_range<512>},       {1024, &l_range<1024>, &prep_range<1024>},
+                          {2048, &l_range<2048>, &prep_range<2048>},    {4096, &l_range<4096>, &prep_range<4096>},
+                          {8192, &l_range<8192>, &prep_range<8192>},    {16384, &l_range<16384>, &prep_range<16384>}};
+#define MFFT_AZ(N) {N, AzGeom<N>::C, &l_az<N, true, false>, &l_az<N, false, true>, &l_az<N, true, true>, &prep_az<N>}
+const AzK g_az[] = {MFFT_AZ(64), MFFT_AZ(128), MFFT_AZ(256), MFFT_AZ(512), MFFT_AZ(1024), MFFT_AZ(2048), MFFT_AZ(4096)};
+
+const BatchedKernel* e16(int n) {
+    int cnt = 0;
+    const BatchedKernel* ks = batched_kernels(&cnt);
+    for (int i = 0; i < cnt; ++i)
+        if (ks[i].n == n && ks[i].e == 16) return &ks[i];
+    return nullptr;
+}
+
+}  // namespace
+}  // namespace mfft
+
+using namespace mfft;
+
+struct mfft_sar {
+    mfft_ctx* ctx = nullptr;
+    mfft_sar_params prm{};
+    const RangeK* rk = nullptr;
+    const AzK* ak = nullptr;
+    float2* tw_r = nullptr;
+    float2* tw_a = nullptr;
+    float2* H = nullptr;
+    __half2* rc = nullptr;  // range-compressed pulses, FP16 pulse-major
+    float* rc_scale = nullptr;
+    float* dphi_part = nullptr;
+    double* loss_part = nullptr;
+    long long tiles = 0;
+    cudaGraphExec_t graph = nullptr;
+    const void* g_key[8] = {};
+};
+
+static int check_params(const mfft_sar_params* p) {
+    if (!p) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "params is NULL");
+    if (!is_pow2_in(p->pulses, 64, 4096))
+        return set_error(MFFT_ERR_UNSUPPORTED_SIZE, p->pulses, -1, -1, "pulses must be a power of two 64..4096, got %lld",
+                         (long long)p->pulses);
+    if (!is_pow2_in(p->range_n, 512, 16384))
+        return set_error(MFFT_ERR_UNSUPPORTED_SIZE, p->range_n, -1, -1,
+                         "range_n must be a power of two 512..16384, got %lld", (long long)p->range_n);
+    if (p->chirp_samples < 1 || p->chirp_samples > p->range_n || !(p->sample_rate > 0) || !(p->prf > 0) ||
+        !(p->bandwidth > 0) || !(p->carrier > 0))
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "invalid SAR parameters");
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_sar_default_params(int64_t pulses, int64_t range_n, int64_t chirp_samples, double tbp,
+                                       mfft_sar_params* out) {
+    if (!out || chirp_samples < 1 || !(tbp > 0)) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "bad arguments");
+    out->pulses = pulses;
+    out->range_n = range_n;
+    out->chirp_samples = chirp_samples;
+    out->bandwidth = 100e6;
+    out->sample_rate = (double)chirp_samples * out->bandwidth / tbp;  // Tp*fs = samples, B*Tp = tbp
+    out->prf = 1000.0;
+    out->velocity = 100.0;
+    out->carrier = 10e9;
+    out->center_range = 20000.0;
+    return check_params(out);
+}
+
+extern "C" int mfft_sar_chirp_reference(const mfft_sar_params* p, void* chirp) {
+    int st = check_params(p);
+    if (st) return st;
+    if (!chirp) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "chirp is NULL");
+    const SarGeom g = make_geom(*p);
+    float2* out = (float2*)chirp;
+    for (int64_t i = 0; i < p->range_n; ++i) out[i] = make_float2(0.f, 0.f);
+    const int64_t ns = p->chirp_samples, half = ns / 2;
+    for (int64_t i = 0; i < ns; ++i) {
+        const double t = (double)(i - half) / p->sample_rate;
+        const double ph = PI_D * g.kr * t * t;
+        const int64_t idx = i < half ? p->range_n - half + i : i - half;
+        if (idx < p->range_n) out[idx] = make_float2((float)cos(ph), (float)sin(ph));
+    }
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_sar_simulate(mfft_ctx* ctx, const mfft_sar_params* p, const mfft_sar_target* targets,
+                                 int ntargets, double snr_db, uint64_t seed, void* raw, void* stream) {
+    int st = check_params(p);
+    if (st) return st;
+    if (!raw || ntargets < 0 || (ntargets > 0 && !targets))
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "bad simulator arguments");
+    if (!ctx) {
+        st = mfft_context_shared(&ctx);
+        if (st) return st;
+    }
+    DeviceGuard gd(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const SarGeom g = make_geom(*p);
+    const long long n = g.na * g.nr;
+    mfft_sar_target* dt = nullptr;
+    double* part = nullptr;
+    const int nparts = 1024;
+    cudaError_t e = cudaMallocAsync(&dt, sizeof(mfft_sar_target) * (ntargets > 0 ? ntargets : 1), s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&part, sizeof(double) * 2 * nparts, s);
+    if (e != cudaSuccess) return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "simulator buffers: %s", cudaGetErrorString(e));
+    if (ntargets > 0) e = cudaMemcpyAsync(dt, targets, sizeof(mfft_sar_target) * ntargets, cudaMemcpyHostToDevice, s);
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    k_sar_signal<<<blocks, 256, 0, s>>>((float2*)raw, g, dt, ntargets);
+    k_sar_power<<<nparts, 256, 0, s>>>((const float2*)raw, n, part);
+    k_sar_noise<<<blocks, 256, 0, s>>>((float2*)raw, n, part, nparts, snr_db, seed);
+    cudaFreeAsync(dt, s);
+    cudaFreeAsync(part, s);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_error(e, "SAR simulator");
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_sar_quantize(mfft_ctx* ctx, int64_t pulses, int64_t range_n, const void* raw, void* raw_h,
+                                 float* pulse_scale, void* stream) {
+    if (!raw || !raw_h || !pulse_scale || pulses < 1 || range_n < 1)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "bad quantize arguments");
+    if (!ctx) {
+        int st = mfft_context_shared(&ctx);
+        if (st) return st;
+    }
+    DeviceGuard gd(ctx->device);
+    k_sar_quantize<<<(unsigned)pulses, 256, 0, (cudaStream_t)stream>>>((const float2*)raw, range_n, (__half2*)raw_h,
+                                                                       pulse_scale);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_error(e, "SAR quantize");
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_sar_destroy(mfft_sar* s) {
+    if (!s) return MFFT_SUCCESS;
+    DeviceGuard gd(s->ctx->device);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    cudaFree(s->H);
+    cudaFree(s->rc);
+    cudaFree(s->rc_scale);
+    cudaFree(s->dphi_part);
+    cudaFree(s->loss_part);
+    delete s;
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_sar_create(mfft_ctx* ctx, const mfft_sar_params* p, const void* chirp_ref, mfft_sar** out) {
+    if (!out) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "out is NULL");
+    *out = nullptr;
+    int st = check_params(p);
+    if (st) return st;
+    if (!chirp_ref) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "chirp_ref is NULL");
+    if (!ctx) {
+        st = mfft_context_shared(&ctx);
+        if (st) return st;
+    }
+    DeviceGuard gd(ctx->device);
+    mfft_sar* s = new mfft_sar();
+    s->ctx = ctx;
+    s->prm = *p;
+    for (const auto& k : g_range)
+        if (k.n == p->range_n) s->rk = &k;
+    for (const auto& k : g_az)
+        if (k.n == p->pulses) s->ak = &k;
+    s->tiles = p->range_n / s->ak->cols;
+    BatchedBinding br, ba;
+    st = bind_batched(ctx, e16((int)p->range_n), &br);
+    if (!st) st = bind_batched(ctx, e16((int)p->pulses), &ba);
+    s->tw_r = br.tw;
+    s->tw_a = ba.tw;
+    cudaError_t e = cudaSuccess;
+    if (!st) {
+        e = s->rk->prep();
+        if (e == cudaSuccess) e = s->ak->prep();
+        if (e != cudaSuccess) st = cuda_error(e, "SAR kernel attributes");
+    }
+    const long long na = p->pulses, nr = p->range_n;
+    if (!st) {
+        e = cudaMalloc(&s->H, sizeof(float2) * nr * 2);
+        if (e == cudaSuccess) e = cudaMalloc(&s->rc, sizeof(__half2) * na * nr);
+        if (e == cudaSuccess) e = cudaMalloc(&s->rc_scale, sizeof(float) * na);
+        if (e == cudaSuccess) e = cudaMalloc(&s->dphi_part, sizeof(float) * s->tiles * na);
+        if (e == cudaSuccess) e = cudaMalloc(&s->loss_part, sizeof(double) * s->tiles);
+        if (e != cudaSuccess) st = set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "SAR buffers: %s", cudaGetErrorString(e));
+    }
+    if (!st) {
+        // H = conj(FFT(chirp_ref)): conj(FFT(c)) computed as the inverse-scaled
+        // transform of conj(c) would change the scale, so transform and conjugate
+        std::vector<float2> h((size_t)nr);
+        memcpy(h.data(), chirp_ref, sizeof(float2) * nr);
+        float2* tmp = s->H + nr;
+        e = cudaMemcpyAsync(tmp, h.data(), sizeof(float2) * nr, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = br.k->fwd(tmp, s->H, 1, br.tw, ctx->dev_err, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), s->H, sizeof(float2) * nr, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        for (auto& v : h) v.y = -v.y;
+        if (e == cudaSuccess) e = cudaMemcpy(s->H, h.data(), sizeof(float2) * nr, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) st = cuda_error(e, "range matched filter");
+    }
+    if (st) {
+        mfft_sar_destroy(s);
+        return st;
+    }
+    *out = s;
+    return MFFT_SUCCESS;
+}
+
+static int sar_pass_a(mfft_sar* s, const void* raw_h, const float* ps, const float* ph, cudaStream_t st) {
+    s->rk->f((int)s->prm.pulses, st, (const __half2*)raw_h, ps, ph, s->H, s->tw_r, s->rc, s->rc_scale);
+    return MFFT_SUCCESS;
+}
+
+static int sar_check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? (int)MFFT_SUCCESS : cuda_error(e, what);
+}
+
+extern "C" int mfft_sar_forward(mfft_sar* s, const void* raw_h, const float* pulse_scale, const float* phase,
+                                void* image_h, float* image_scale, void* stream) {
+    if (!s || !raw_h || !pulse_scale || !phase || !image_h || !image_scale)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "NULL argument");
+    DeviceGuard gd(s->ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    sar_pass_a(s, raw_h, pulse_scale, phase, st);
+    s->ak->fwd((int)s->tiles, st, s->rc, s->rc_scale, s->prm.range_n, s->tw_a, (__half2*)image_h, image_scale, nullptr,
+               nullptr);
+    return sar_check_launch("SAR forward");
+}
+
+extern "C" int mfft_sar_backward_phase(mfft_sar* s, const void* raw_h, const float* pulse_scale, const float* phase,
+                                       float* dphi, double* loss, void* stream) {
+    if (!s || !raw_h || !pulse_scale || !phase || !dphi)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "NULL argument");
+    DeviceGuard gd(s->ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    sar_pass_a(s, raw_h, pulse_scale, phase, st);
+    s->ak->bwd((int)s->tiles, st, s->rc, s->rc_scale, s->prm.range_n, s->tw_a, nullptr, nullptr, s->dphi_part,
+               s->loss_part);
+    k_sar_reduce<<<(unsigned)((s->prm.pulses + 255) / 256), 256, 0, st>>>(s->dphi_part, s->tiles, s->prm.pulses, dphi,
+                                                                          s->loss_part, loss);
+    return sar_check_launch("SAR backward");
+}
+
+static void sar_enqueue_step(mfft_sar* s, const void* raw_h, const float* ps, const float* ph, void* image_h,
+                             float* image_scale, float* dphi, double* loss, cudaStream_t st) {
+    sar_pass_a(s, raw_h, ps, ph, st);
+    s->ak->both((int)s->tiles, st, s->rc, s->rc_scale, s->prm.range_n, s->tw_a, (__half2*)image_h, image_scale,
+                s->dphi_part, s->loss_part);
+    k_sar_reduce<<<(unsigned)((s->prm.pulses + 255) / 256), 256, 0, st>>>(s->dphi_part, s->tiles, s->prm.pulses, dphi,
+                                                                          s->loss_part, loss);
+}
+
+extern "C" int mfft_sar_step_graph(mfft_sar* s, const void* raw_h, const float* pulse_scale, const float* phase,
+                                   void* image_h, float* image_scale, float* dphi, double* loss, void* stream) {
+    if (!s || !raw_h || !pulse_scale || !phase || !image_h || !image_scale || !dphi)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "NULL argument");
+    DeviceGuard gd(s->ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const void* key[8] = {raw_h, pulse_scale, phase, image_h, image_scale, dphi, loss, stream};
+    bool same = s->graph != nullptr;
+    for (int i = 0; i < 8 && same; ++i) same = (key[i] == s->g_key[i]);
+    if (!same) {
+        if (s->graph) cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        // capture on a private stream, so a legacy default stream can be used too
+        cudaStream_t cs;
+        cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return set_error(MFFT_ERR_NO_STREAM, -1, -1, -1, "capture stream: %s", cudaGetErrorString(e));
+        cudaGraph_t g = nullptr;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            sar_enqueue_step(s, raw_h, pulse_scale, phase, image_h, image_scale, dphi, loss, cs);
+            e = cudaStreamEndCapture(cs, &g);
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cs);
+        if (e != cudaSuccess) {
+            s->graph = nullptr;
+            return cuda_error(e, "SAR graph capture");
+        }
+        for (int i = 0; i < 8; ++i) s->g_key[i] = key[i];
+    }
+    cudaError_t e = cudaGraphLaunch(s->graph, st);
+    if (e != cudaSuccess) return cuda_error(e, "SAR graph launch");
+    return MFFT_SUCCESS;
+}

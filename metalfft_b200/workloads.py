@@ -35,3 +35,25 @@ def conv_workload(seed=20261203, nx=1 << 24, K=4095, decay=800.0):
     h = (rng.standard_normal(K) * np.exp(-np.arange(K) / decay)).astype(np.float32)
     t = rng.standard_normal(nx + K - 1, dtype=np.float32)
     return x, h, t
+
+
+def sar_targets(params, n=64, seed=20261203):
+    """Config 5 scatterers: seeded range bins inside the chirp margin, seeded
+    azimuth pulses in the middle three quarters, amplitude U[0.1, 1], phase
+    U[0, 2 pi).  Returns a list of metalfft_b200.SARTarget."""
+    from ._sar import SARTarget
+    rng = np.random.default_rng(seed)
+    c = 299792458.0
+    out = []
+    for _ in range(n):
+        rb = int(rng.integers(params.chirp_samples, params.range_n - params.chirp_samples))
+        pb = int(rng.integers(params.pulses // 8, 7 * params.pulses // 8))
+        R0 = c * (params.tau0 + rb / params.sample_rate) / 2.0
+        x = params.velocity * (pb - params.pulses / 2) / params.prf
+        out.append(SARTarget(R0, x, float(rng.uniform(0.1, 1.0)), float(rng.uniform(0.0, 2 * np.pi))))
+    return out
+
+
+def sar_phase(pulses, seed=20261203, sigma=0.3):
+    """Per-pulse phase-error vector ~ N(0, sigma) rad."""
+    return np.random.default_rng(seed + 1).normal(0.0, sigma, pulses).astype(np.float32)

@@ -175,3 +175,59 @@ def normal_c64(shape, seed):
     rng = np.random.default_rng(seed)
     z = rng.standard_normal(size=tuple(shape) + (2,), dtype=np.float32)
     return z.view(np.complex64)[..., 0]
+
+
+# ---- SAR (sar_oracle.c) -------------------------------------------------------
+
+class _SarParams(ctypes.Structure):
+    _fields_ = [("pulses", ctypes.c_int64), ("range_n", ctypes.c_int64), ("chirp_samples", ctypes.c_int64),
+                ("bandwidth", ctypes.c_double), ("sample_rate", ctypes.c_double), ("prf", ctypes.c_double),
+                ("velocity", ctypes.c_double), ("carrier", ctypes.c_double), ("center_range", ctypes.c_double)]
+
+
+class _SarTarget(ctypes.Structure):
+    _fields_ = [("range_m", ctypes.c_double), ("azimuth_m", ctypes.c_double), ("amplitude", ctypes.c_double),
+                ("phase", ctypes.c_double)]
+
+
+def _sar_args(params, targets):
+    p = _SarParams(*(getattr(params, f) for f, _ in _SarParams._fields_))
+    arr = (_SarTarget * max(1, len(targets)))(*[_SarTarget(t.range_m, t.azimuth_m, t.amplitude, t.phase)
+                                                  for t in targets])
+    return p, arr
+
+
+def sar_simulate(params, targets, snr_db, seed):
+    L = load()
+    L.mfo_sar_simulate.restype = None
+    p, arr = _sar_args(params, targets)
+    raw = np.empty((params.pulses, params.range_n), np.complex128)
+    L.mfo_sar_simulate(ctypes.byref(p), arr, len(targets), ctypes.c_double(snr_db), ctypes.c_uint64(seed),
+                       raw.ctypes.data_as(_dp))
+    return raw
+
+
+def sar_image(params, raw, chirp, phi):
+    L = load()
+    L.mfo_sar_image.restype = None
+    p, _ = _sar_args(params, [])
+    raw = np.ascontiguousarray(raw, np.complex128)
+    ch = np.ascontiguousarray(chirp, np.complex128)
+    ph = np.ascontiguousarray(phi, np.float64)
+    img = np.empty((params.pulses, params.range_n), np.complex128)
+    L.mfo_sar_image(ctypes.byref(p), raw.ctypes.data_as(_dp), ch.ctypes.data_as(_dp), ph.ctypes.data_as(_dp),
+                    img.ctypes.data_as(_dp), None)
+    return img
+
+
+def sar_loss_grad(params, raw, chirp, phi):
+    L = load()
+    L.mfo_sar_loss_grad.restype = ctypes.c_double
+    p, _ = _sar_args(params, [])
+    raw = np.ascontiguousarray(raw, np.complex128)
+    ch = np.ascontiguousarray(chirp, np.complex128)
+    ph = np.ascontiguousarray(phi, np.float64)
+    d = np.empty(params.pulses, np.float64)
+    loss = L.mfo_sar_loss_grad(ctypes.byref(p), raw.ctypes.data_as(_dp), ch.ctypes.data_as(_dp),
+                               ph.ctypes.data_as(_dp), d.ctypes.data_as(_dp))
+    return loss, d
