@@ -142,7 +142,9 @@ class ClockSampler:
 
 def make_input(batch, rank):
     import numpy as np
-    rng = np.random.default_rng(SEED + rank)
+
+    from metalfft_b200 import dist as D
+    rng = np.random.default_rng(D.replica_seed(SEED, rank))
     z = rng.standard_normal(size=(batch, N, 2), dtype=np.float32)
     return z.view(np.complex64)[..., 0]
 
@@ -223,10 +225,8 @@ def timed(fn, steps, warmup, barrier, dist, uuid):
         torch.cuda.synchronize()
     barrier()
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item()), ms, clk.summary()
+    from metalfft_b200 import dist as D
+    return D.max_over_ranks(ms, device="cuda"), ms, clk.summary()
 
 
 def run_other(args, M, rank, world, dist, barrier, uuid):
@@ -367,6 +367,7 @@ def main():
             dist.barrier()
 
     import metalfft_b200 as M
+    from metalfft_b200 import dist as D
 
     uuid = None
     try:
@@ -417,10 +418,7 @@ def main():
             torch.cuda.synchronize()
         barrier()
         ms = e0.elapsed_time(e1)
-        t = torch.tensor([ms], device="cuda")
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+        ms_max = D.max_over_ranks(ms, device="cuda")
         per_launch_s = ms / args.steps / 1e3
         gbs = BYTES_PER_TRANSFORM * B / per_launch_s / 1e9
         results[name] = {
@@ -457,11 +455,8 @@ def main():
     for _ in range(args.e2e_steps):
         e2e_call()
     barrier()
-    dt = time.perf_counter() - t0
-    tt = torch.tensor([dt], device="cuda")
-    if dist is not None:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e = {"value": B * world * args.e2e_steps / float(tt.item()), "unit": "transforms/s",
+    dt = D.max_over_ranks(time.perf_counter() - t0, device="cuda")
+    e2e = {"value": B * world * args.e2e_steps / dt, "unit": "transforms/s",
            "h2d_bytes_per_step": B * N * 8, "d2h_bytes_per_step": B * N * 8,
            "steps": args.e2e_steps}
 

@@ -28,7 +28,9 @@
 //
 // One CTA of 256 threads (8 warps) transforms one line at a time, 2 CTAs per
 // SM; the next line's loads are issued before the current line's tensor-core
-// work so they overlap it.  The single thread that issues the MMAs waits on
+// work so they overlap it, and its maximum is published at the barrier that
+// ends the current line.  The stage-2 scale is s1/64 (a DFT-64 grows
+// magnitudes by at most 64), so no reduction sits between the two products.  The single thread that issues the MMAs waits on
 // the commit mbarrier with a time limit; a timeout sets the device error word
 // and the CTA leaves its loop, frees its TMEM and returns.
 #include "capi_internal.h"
@@ -53,7 +55,9 @@ constexpr uint32_t SM_G0 = 0;          // G hi (or bf16) : 128 x 128 halves = 32
 constexpr uint32_t SM_G1 = 32768;      // G lo
 constexpr uint32_t SM_B0 = 65536;      // B hi (or bf16) : 128 x 64 halves = 16 KB
 constexpr uint32_t SM_B1 = 81920;      // B lo
-constexpr uint32_t SM_BYTES = 98304 + 1024;  // + alignment slack
+constexpr uint32_t SM_T1 = 98304;      // W4096^(i*k1), i < 16, k1 < 64: 8 KB
+constexpr uint32_t SM_T0 = 106496;     // W4096^(16*j*k1), j < 4, k1 < 64: 2 KB
+constexpr uint32_t SM_BYTES = 108544 + 1024;  // + alignment slack
 constexpr uint32_t TMEM_COLS = 128;    // D1: columns [0, 64), D2: [64, 128)
 
 // Operand layouts: 128-byte swizzle (1024-byte atoms of 8 rows x 128 bytes,
@@ -112,17 +116,6 @@ __device__ __forceinline__ float line_scale(float mx) {
     return ldexpf(1.f, TC_LINE_EXP - e);
 }
 
-__device__ __forceinline__ float block_max(float v, float* red, int tid) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((tid & 31) == 0) red[tid >> 5] = v;
-    __syncthreads();
-    float m = red[0];
-#pragma unroll
-    for (int w = 1; w < TC_THREADS / 32; ++w) m = fmaxf(m, red[w]);
-    return m;
-}
-
 // 8 values -> one 16-byte chunk of hi (and lo) halves / bf16
 template <bool SPLIT>
 __device__ __forceinline__ void store_chunk(uint8_t* smem, uint32_t off, const float (&x)[8]) {
@@ -172,7 +165,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base_sh;
-    __shared__ float red1[TC_THREADS / 32], red2[TC_THREADS / 32];
+    __shared__ float red1[TC_THREADS / 32];
     __shared__ int abort_sh;
 
     const int tid = threadIdx.x;
@@ -188,6 +181,12 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
     constexpr int GWORDS = (SPLIT ? 65536 : 32768) / 16;
     for (int i = tid; i < GWORDS; i += TC_THREADS)
         reinterpret_cast<uint4*>(smem)[i] = __ldg(gimg + i);
+    // stage twiddles W4096^(n2*k1), n2 = 16*j + i: T0[j][k1] * T1[i][k1], so a
+    // warp (consecutive k1) reads consecutive shared-memory words
+    float2* t1 = reinterpret_cast<float2*>(smem + SM_T1);
+    float2* t0 = reinterpret_cast<float2*>(smem + SM_T0);
+    for (int i = tid; i < 16 * 64; i += TC_THREADS) t1[i] = __ldg(tw + ((i >> 6) * (i & 63)));
+    for (int i = tid; i < 4 * 64; i += TC_THREADS) t0[i] = __ldg(tw + (16 * (i >> 6) * (i & 63)));
     if (tid == 0) {
         mbar_init(&mbar, 1);
         abort_sh = 0;
@@ -218,21 +217,41 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
             for (int j = 0; j < 4; ++j) cur[4 * it + j] = __ldcs(src + 4 * (tid + TC_THREADS * it) + j);
     };
 
-    uint32_t phase = 0;
-    long long f = blockIdx.x;
-    if (f < batch) load_line(f);
-    for (; f < batch; f += gridDim.x) {
-        // ---- stage-1 operand: scale, split, write B (MN-major) ----
+    // per-warp partial max of the line in `cur`, published through red1 by
+    // the barrier that precedes its use
+    auto publish_max = [&]() {
         float mx = 0.f;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            if constexpr (INV) {
+        for (int i = 0; i < 8; ++i)
+            mx = fmaxf(mx, fmaxf(fmaxf(fabsf(cur[i].x), fabsf(cur[i].y)), fmaxf(fabsf(cur[i].z), fabsf(cur[i].w))));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) red1[warp] = mx;
+    };
+
+    uint32_t phase = 0;
+    long long f = blockIdx.x;
+    if (f < batch) {
+        load_line(f);
+        if constexpr (SPLIT) publish_max();
+    }
+    __syncthreads();
+    for (; f < batch; f += gridDim.x) {
+        // ---- stage-1 operand: scale, split, write B (MN-major) ----
+        if constexpr (INV) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
                 cur[i].y = -cur[i].y;
                 cur[i].w = -cur[i].w;
             }
-            mx = fmaxf(mx, fmaxf(fmaxf(fabsf(cur[i].x), fabsf(cur[i].y)), fmaxf(fabsf(cur[i].z), fabsf(cur[i].w))));
         }
-        const float s1 = SPLIT ? line_scale(block_max(mx, red1, tid)) : 1.f;
+        float s1 = 1.f;
+        if constexpr (SPLIT) {
+            float m = red1[0];
+#pragma unroll
+            for (int w = 1; w < TC_THREADS / 32; ++w) m = fmaxf(m, red1[w]);
+            s1 = line_scale(m);
+        }
 #pragma unroll
         for (int it = 0; it < 2; ++it) {
             const int item = tid + TC_THREADS * it;  // (n1, c): n2 = 8c .. 8c+7
@@ -282,15 +301,14 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
             }
         }
         const int n2_0 = 32 * h + 16 * bsel;  // this thread's n2 range; k1 = kk_
-        float mx2 = 0.f;
+        {
+            const float2 w0 = t0[(n2_0 >> 4) * 64 + kk_];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-            const int e = ((n2_0 + i) * kk_) & (TC_N - 1);
-            z[i] = cmul(z[i], __ldg(tw + e));
-            mx2 = fmaxf(mx2, fmaxf(fabsf(z[i].x), fabsf(z[i].y)));
+            for (int i = 0; i < 16; ++i) z[i] = cmul(z[i], cmul(w0, t1[i * 64 + kk_]));
         }
-        tc::fence_before_sync();
-        const float s2 = SPLIT ? line_scale(block_max(mx2, red2, tid)) : 1.f;
+        // a DFT-64 grows magnitudes by at most 64: s1 / 64 keeps |Z| s2 < 2^14
+        // without a second reduction over the line
+        const float s2 = SPLIT ? s1 * (1.f / 64.f) : 1.f;
         {
             // K-major row nn = k1, K = 2*n2 + a: 4 chunks of 8 (4 complex values)
 #pragma unroll
@@ -345,8 +363,11 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 #pragma unroll
             for (int i = 0; i < 8; ++i) __stcs(dst + i, o[i]);
         }
+        if constexpr (SPLIT) {
+            if (f + gridDim.x < batch) publish_max();  // the prefetched line
+        }
         tc::fence_before_sync();
-        __syncthreads();  // TMEM and B are free for the next line
+        __syncthreads();  // TMEM and B are free for the next line; red1 published
     }
 
     if (abort_sh && tid == 0) {
