@@ -148,6 +148,11 @@ MFFT_API int mfft_autotune(mfft_ctx* ctx, int64_t n, int64_t lines, int* radix, 
 /* Pins a plan (n <= 16384) to one registered variant.
  * MFFT_ERR_KERNEL_NOT_FOUND if that variant is not built. */
 MFFT_API int mfft_plan_set_kernel(mfft_plan* plan, int radix, int lines_per_cta, int stages);
+/* Four-step plans (n > 16384): how many lines one column pass + row pass
+ * covers (the intermediate of a chunk is lines * n complex values).  Smaller
+ * chunks keep the intermediate resident in L2 between the two passes; the
+ * plan's scratch is reallocated when the chunk grows.  lines >= 1. */
+MFFT_API int mfft_plan_set_fourstep_chunk(mfft_plan* plan, int64_t lines);
 /* Lists the registered variants for size n: fills up to cap entries and
  * returns how many exist (host only). */
 MFFT_API int mfft_list_kernels(int64_t n, int* radix, int* lines_per_cta, int* stages, int cap);

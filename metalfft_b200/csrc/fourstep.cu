@@ -246,3 +246,22 @@ int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, in
 }
 
 }  // namespace mfft
+
+extern "C" int mfft_plan_set_fourstep_chunk(mfft_plan* plan, int64_t lines) {
+    using namespace mfft;
+    if (!plan) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "plan is NULL");
+    if (plan->n <= MFFT_MAX_SINGLE_N)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "n=%lld has no four-step chunk", (long long)plan->n);
+    if (lines < 1) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, lines, -1, "lines must be >= 1");
+    DeviceGuard g(plan->ctx->device);
+    FourStep& fs = plan->fs;
+    if (lines > fs.scratch_lines) {
+        float2* s = nullptr;
+        cudaError_t e = cudaMalloc(&s, sizeof(float2) * (size_t)lines * (size_t)plan->n);
+        if (e != cudaSuccess) return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "four-step scratch: %s", cudaGetErrorString(e));
+        cudaFree(fs.scratch);
+        fs.scratch = s;
+    }
+    fs.scratch_lines = lines;
+    return MFFT_SUCCESS;
+}
