@@ -158,6 +158,19 @@ class MetalFFT:
         _check(st)
         return out
 
+    def capture(self, calls):
+        """One CUDA graph of device-tensor execs.  `calls` is a list of
+        (inp, out, batch, direction) or (inp, out, batch, direction,
+        tc_variant); the returned torch.cuda.CUDAGraph re-runs all of them
+        with one replay(), so a small batch costs one graph launch instead of
+        one host call per kernel.  The tensors must stay alive and in place."""
+        import torch
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for c in calls:
+                self.exec(*c)
+        return g
+
     def _run(self, x, batch, direction, tc_variant=0):
         if _is_cuda_tensor(x):
             import torch
