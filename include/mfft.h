@@ -22,7 +22,10 @@
  *    Swift arrays' semantics (MetalFFT.swift:74-84, synchronous like
  *    commitAndWait, Internal/Dispatch.swift:3-10).  MFFT_DEVICE_MEMORY means
  *    the pointers are device memory and the work is only enqueued on
- *    `stream` (a cudaStream_t; NULL = the legacy default stream).
+ *    `stream` (a cudaStream_t; NULL = the legacy default stream).  Complex
+ *    device buffers of the FFT calls (mfft_exec_c2c, mfft_exec_c2c_tc,
+ *    mfft_multi_exec) must be 16-byte aligned, as cudaMalloc and PyTorch
+ *    allocations are; others are MFFT_ERR_INVALID_ARGUMENT.
  *  - Handles are single-writer: one thread at a time per handle
  *    (MetalFFT.swift:9).  Context creation is thread-safe.
  */
@@ -148,11 +151,6 @@ MFFT_API int mfft_autotune(mfft_ctx* ctx, int64_t n, int64_t lines, int* radix, 
 /* Pins a plan (n <= 16384) to one registered variant.
  * MFFT_ERR_KERNEL_NOT_FOUND if that variant is not built. */
 MFFT_API int mfft_plan_set_kernel(mfft_plan* plan, int radix, int lines_per_cta, int stages);
-/* Four-step plans (n > 16384): how many lines one column pass + row pass
- * covers (the intermediate of a chunk is lines * n complex values).  Smaller
- * chunks keep the intermediate resident in L2 between the two passes; the
- * plan's scratch is reallocated when the chunk grows.  lines >= 1. */
-MFFT_API int mfft_plan_set_fourstep_chunk(mfft_plan* plan, int64_t lines);
 /* Lists the registered variants for size n: fills up to cap entries and
  * returns how many exist (host only). */
 MFFT_API int mfft_list_kernels(int64_t n, int* radix, int* lines_per_cta, int* stages, int cap);
@@ -196,9 +194,11 @@ MFFT_API int mfft_fourstep_noalloc(const void* in, void* out, int64_t n, int64_t
 /* ---- mixed sizes in one persistent launch ------------------------------ */
 
 /* One size class: `count` transforms of length n (power of two, 64..2^20)
- * stored back to back starting at complex element `offset` of the in/out
- * buffers.  There is no reference counterpart for a single launch over mixed
- * sizes; it generalises forward(batch:) (MetalFFT.swift:108-133). */
+ * stored back to back starting at complex element `offset` (even) of the
+ * in/out buffers.  There is no reference counterpart for a single launch over
+ * mixed sizes; it generalises forward(batch:) (MetalFFT.swift:108-133).
+ * Sizes up to 4096 run as whole lines, larger ones as four-step transforms
+ * whose intermediates stay in a small L2-resident scratch ring. */
 typedef struct mfft_multi_desc {
     int64_t n;
     int64_t count;

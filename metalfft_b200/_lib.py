@@ -33,7 +33,6 @@ SIGNATURES = [
     ("mfft_autotune", c_int, [c_void_p, c_int64, c_int64, P(c_int), P(c_int), P(c_int)]),
     ("mfft_plan_kernel_info", c_int, [c_void_p, P(c_int), P(c_int), P(c_int), P(c_int)]),
     ("mfft_plan_set_kernel", c_int, [c_void_p, c_int, c_int, c_int]),
-    ("mfft_plan_set_fourstep_chunk", c_int, [c_void_p, c_int64]),
     ("mfft_list_kernels", c_int, [c_int64, P(c_int), P(c_int), P(c_int), c_int]),
     ("mfft_exec_c2c", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),
     ("mfft_exec_c2c_tc", c_int,

@@ -316,6 +316,9 @@ int check_exec_args(const void* in, void* out, int64_t batch, int direction, int
     if (flags != MFFT_HOST_MEMORY && flags != MFFT_DEVICE_MEMORY)
         return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "unknown flags %d", flags);
     if (batch > 0 && (!in || !out)) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "NULL buffer");
+    // the kernels move 16-byte chunks (bulk copies, cp.async, vector stores)
+    if (flags == MFFT_DEVICE_MEMORY && (((uintptr_t)in | (uintptr_t)out) & 15))
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "device buffers must be 16-byte aligned");
     return MFFT_SUCCESS;
 }
 

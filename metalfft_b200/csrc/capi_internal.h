@@ -33,15 +33,14 @@ struct BatchedBinding {
     float2* tw = nullptr;
 };
 
-// Four-step state for n > 16384 (n = n1 * n2, both <= 16384).
+// Four-step state for n > 16384 (n = n1 * n2, n1 <= n2 <= 1024), run by the
+// item kernel of fsqueue.cu.
 struct FourStep {
     int n1 = 0, n2 = 0;
-    const void* col = nullptr;   // column-pass kernel descriptor
-    const void* row = nullptr;   // row-pass kernel descriptor
-    float2* col_tw = nullptr;
+    float2* col_tw = nullptr;    // line twiddle rows for n1 and n2
     float2* row_tw = nullptr;
     float2* tables = nullptr;    // W_N^m = fine[m % 1024] * coarse[m / 1024]
-    float2* scratch = nullptr;   // intermediate, scratch_lines * n float2
+    float2* scratch = nullptr;   // intermediates of up to scratch_lines transforms
     long long scratch_lines = 0;
 };
 
@@ -85,6 +84,12 @@ int check_device_error(mfft_ctx* ctx);
 // in_place: the kernels may read and write one buffer (batched FFTs).
 int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, size_t out_bytes,
                     const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body, bool in_place = false);
+
+// Line twiddle rows (E = 16) of size n, cached in the context.
+int line_twiddles(mfft_ctx* ctx, int n, float2** out);
+// W_n^m tables (fine[1024] then coarse[n / 1024]) for a four-step size n,
+// built on the context's stream; the caller owns the allocation.
+int fourstep_tables(mfft_ctx* ctx, int64_t n, float2** out);
 
 int fourstep_plan_init(mfft_plan* plan);
 void fourstep_plan_release(mfft_plan* plan);

@@ -1,0 +1,333 @@
+// fsqueue.cu -- the persistent item kernel (item kinds and passes in
+// fsqueue.h).
+//
+// B200 form of the reference's batched and four-step dispatches
+// (Sources/MetalFFT/FFT/MetalFFT.swift:159-277: one threadgroup per line, or
+// five encoders and three scalar transposes per four-step transform, one
+// command buffer per batch element).  Here one launch runs a whole pass:
+//  * every item moves with 16-byte cp.async copies into the stage buffer the
+//    CTA is not computing on, so DRAM traffic overlaps the FFT arithmetic;
+//    the schedule is static, so the next item is always known and no CTA
+//    ever waits for another;
+//  * the row pass reads each intermediate once and then discards its lines
+//    from L2 (discard.global.L2), so a dead intermediate still in L2 is never
+//    written back to DRAM;
+//  * the column tiles and the transposed row-pass output go through shared
+//    memory in 16-byte chunks with an XOR swizzle on chunk pairs, so global
+//    accesses are whole 32-byte sectors and shared-memory reads stay within
+//    two wavefronts of the minimum.
+// Each line transform is the in-register radix-16 Stockham FFT of
+// stockham.cuh (padded exchange, one line, column or row per T = n/16
+// threads, t fastest).
+#include "fsqueue.h"
+#include "stockham.cuh"
+#include "tma.cuh"
+
+namespace mfft {
+
+namespace {
+
+constexpr int QSTAGE = spad_size(FSQ_POINTS);  // float2 per stage buffer (4352)
+constexpr int QSMEM = 2 * QSTAGE * (int)sizeof(float2);
+
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// 16-byte global -> shared copy that bypasses L1 (streamed data is read once).
+__device__ __forceinline__ void cp_async16(float2* sdst, const float2* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async16_hint(float2* sdst, const float2* gsrc, uint64_t pol) {
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(smem_u32(sdst)), "l"(gsrc),
+                 "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void discard_l2_line(const void* p) {
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
+// Element (row i, column c) of a tile 2^lw columns wide: rows are 2^lw
+// consecutive slots, and the 16-byte column pairs of row i are permuted by
+// XOR with the index of the 128-byte window row i starts in, so rows that
+// would share banks when a warp walks down a column sit on different pairs.
+__device__ __forceinline__ int pair_swz(int i, int lw) {
+    const int sh = lw < 4 ? 4 - lw : 0;  // rows per 128 bytes = 2^sh
+    return (i >> sh) & ((1 << (lw - 1)) - 1);
+}
+__device__ __forceinline__ int tidx(int i, int c, int lw) {
+    return (i << lw) + ((((c >> 1) ^ pair_swz(i, lw)) << 1) | (c & 1));
+}
+
+// 2^lr rows x 2^lw columns of a row-major array (row stride `stride`) ->
+// stage, in the tidx layout.
+__device__ __forceinline__ void load_tile(float2* st, const float2* g, int lr, int lw, long long stride,
+                                          uint64_t pol) {
+    const int lp = lw - 1, pm = (1 << lp) - 1;
+    const int chunks = 1 << (lr + lp);
+    for (int q = threadIdx.x; q < chunks; q += FSQ_THREADS) {
+        const int i = q >> lp, p = q & pm;
+        cp_async16_hint(st + (i << lw) + ((p ^ pair_swz(i, lw)) << 1), g + i * stride + 2 * p, pol);
+    }
+}
+
+template <bool STREAM>
+__device__ __forceinline__ void store_tile(const float2* st, float2* g, int lr, int lw, long long stride) {
+    const int lp = lw - 1, pm = (1 << lp) - 1;
+    const int chunks = 1 << (lr + lp);
+    for (int q = threadIdx.x; q < chunks; q += FSQ_THREADS) {
+        const int i = q >> lp, p = q & pm;
+        const float4 v = *reinterpret_cast<const float4*>(st + (i << lw) + ((p ^ pair_swz(i, lw)) << 1));
+        float4* dst = reinterpret_cast<float4*>(g + i * stride + 2 * p);
+        if constexpr (STREAM) __stcs(dst, v);
+        else *dst = v;
+    }
+}
+
+// `count` (even) contiguous points -> stage
+__device__ __forceinline__ void load_linear(float2* st, const float2* g, int count, bool hint, uint64_t pol) {
+    for (int q = threadIdx.x; q < count / 2; q += FSQ_THREADS) {
+        if (hint) cp_async16_hint(st + 2 * q, g + 2 * q, pol);
+        else cp_async16(st + 2 * q, g + 2 * q);
+    }
+}
+
+// ---- the three item kinds ---------------------------------------------------
+
+template <int L, bool INV>
+__device__ __forceinline__ void do_lines(float2* st, float2* __restrict__ out, long long off, int lines,
+                                         const float2* __restrict__ tw) {
+    constexpr int T = L / 16;
+    const int u = threadIdx.x / T, t = threadIdx.x % T;
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        v[m] = st[u * L + t + m * T];
+        if constexpr (INV) v[m].y = -v[m].y;
+    }
+    __syncthreads();  // the raw item is in registers; the stage becomes the exchange area
+    fft_regs<L, 16, (T <= 32)>(v, t, PadLine{st + u * spad_size(L)}, tw);
+    if (u < lines) {
+        float2* dst = out + off + (long long)u * L + t;
+        const float s = 1.0f / (float)L;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) __stcs(dst + m * T, INV ? make_float2(v[m].x * s, -v[m].y * s) : v[m]);
+    }
+}
+
+__device__ __forceinline__ float2 tw_n(const float2* __restrict__ fine, const float2* __restrict__ coarse,
+                                       unsigned e) {
+    return cmul(__ldg(fine + (e & 1023u)), __ldg(coarse + (e >> 10)));
+}
+
+template <int L, bool INV>
+__device__ __forceinline__ void do_cols(float2* st, float2* __restrict__ mid, int ln2, int col0,
+                                        const float2* __restrict__ tw, const float2* __restrict__ fine,
+                                        const float2* __restrict__ coarse) {
+    constexpr int T = L / 16, C = FSQ_POINTS / L, LC = ilog2c(C), LL = ilog2c(L);
+    const int c = threadIdx.x / T, t = threadIdx.x % T;
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        v[m] = st[tidx(t + m * T, c, LC)];
+        if constexpr (INV) v[m].y = -v[m].y;
+    }
+    __syncthreads();
+    fft_regs<L, 16, (T <= 32)>(v, t, PadLine{st + c * spad_size(L)}, tw);
+    // W_n^{col*k1}, k1 = t + m*T: base W^{col*t} times W^{col*T*m}, the latter
+    // a product of at most four of W^{col*T*{1,2,4,8}} (warp-uniform loads);
+    // every exponent stays below n
+    {
+        const unsigned col = (unsigned)(col0 + c), step = col * (unsigned)T;
+        const float2 base = tw_n(fine, coarse, col * (unsigned)t);
+        const float2 s1 = tw_n(fine, coarse, step), s2 = tw_n(fine, coarse, 2 * step);
+        const float2 s4 = tw_n(fine, coarse, 4 * step), s8 = tw_n(fine, coarse, 8 * step);
+        float2 u[4];
+        u[0] = base;
+        u[1] = cmul(base, s1);
+        u[2] = cmul(base, s2);
+        u[3] = cmul(u[1], s2);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float2 w4 = cmul(u[q], s4);
+            v[q] = cmul(v[q], u[q]);
+            v[q + 8] = cmul(v[q + 8], cmul(u[q], s8));
+            v[q + 4] = cmul(v[q + 4], w4);
+            v[q + 12] = cmul(v[q + 12], cmul(w4, s8));
+        }
+    }
+    __syncthreads();  // every exchange read is done before the output tile overwrites the stage
+#pragma unroll
+    for (int m = 0; m < 16; ++m) st[tidx(t + m * T, c, LC)] = v[m];
+    __syncthreads();
+    store_tile<false>(st, mid + col0, LL, LC, 1LL << ln2);
+}
+
+template <int L, bool INV>
+__device__ __forceinline__ void do_rows(float2* st, const float2* mid_rows, float2* __restrict__ out, int ln1,
+                                        int row0, const float2* __restrict__ tw, float scale) {
+    constexpr int T = L / 16, RW = FSQ_POINTS / L, LR = ilog2c(RW), LL = ilog2c(L);
+    const int r = threadIdx.x / T, t = threadIdx.x % T;
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = st[r * L + t + m * T];
+    // the intermediate rows now live on chip: drop them from L2 without a
+    // write-back (32 KiB = 256 lines of 128 bytes, one per thread)
+    discard_l2_line(reinterpret_cast<const char*>(mid_rows) + 128 * threadIdx.x);
+    __syncthreads();
+    fft_regs<L, 16, (T <= 32)>(v, t, PadLine{st + r * spad_size(L)}, tw);
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 16; ++m)
+        st[tidx(t + m * T, r, LR)] = INV ? make_float2(v[m].x * scale, -v[m].y * scale) : v[m];
+    __syncthreads();
+    store_tile<true>(st, out + row0, LL, LR, 1LL << ln1);
+}
+
+// ---- items ----------------------------------------------------------------------
+
+struct Work {
+    int kind, logn, index, lines;
+    long long off;      // LINES: first line; COLS / ROWS: the transform in in / out
+    long long scratch;  // COLS / ROWS: the transform's intermediate
+};
+
+__device__ __forceinline__ Work get_work(const FsqArgs& a, int p) {
+    Work w;
+    if (a.items) {
+        const FsqItem it = a.items[p];
+        w.kind = it.kind;
+        w.logn = it.logn;
+        w.index = it.index;
+        w.lines = it.lines;
+        w.off = it.off;
+        w.scratch = 0;
+        if (it.kind != FSQ_LINES) {
+            const FsqXform x = a.xf[it.xform];
+            w.off = x.off;
+            w.scratch = x.scratch;
+        }
+        return w;
+    }
+    const unsigned j = (unsigned)p / (unsigned)a.u_per;
+    w.kind = a.u_kind;
+    w.logn = a.u_logn;
+    w.index = p - (int)(j * (unsigned)a.u_per);
+    w.lines = 0;
+    w.off = (long long)j << a.u_logn;
+    w.scratch = w.off;
+    return w;
+}
+
+__device__ __forceinline__ void issue(const FsqArgs& a, const Work& w, float2* st, uint64_t pol) {
+    if (w.kind == FSQ_LINES) {
+        load_linear(st, a.in + w.off, w.lines << w.logn, true, pol);
+        return;
+    }
+    const int l1 = w.logn / 2, l2 = w.logn - l1;
+    if (w.kind == FSQ_COLS) {
+        const int lc = ilog2c(FSQ_POINTS) - l1;
+        load_tile(st, a.in + w.off + ((long long)w.index << lc), l1, lc, 1LL << l2, pol);
+    } else {
+        const int lr = ilog2c(FSQ_POINTS) - l2;
+        load_linear(st, a.scratch + w.scratch + ((long long)w.index << (lr + l2)), FSQ_POINTS, true, pol);
+    }
+}
+
+template <bool INV>
+__device__ __forceinline__ void compute(const FsqArgs& a, const Work& w, float2* st) {
+    if (w.kind == FSQ_LINES) {
+        const float2* tw = a.tabs.line_tw[w.logn - 6];
+        switch (w.logn) {
+            case 6: do_lines<64, INV>(st, a.out, w.off, w.lines, tw); break;
+            case 7: do_lines<128, INV>(st, a.out, w.off, w.lines, tw); break;
+            case 8: do_lines<256, INV>(st, a.out, w.off, w.lines, tw); break;
+            case 9: do_lines<512, INV>(st, a.out, w.off, w.lines, tw); break;
+            case 10: do_lines<1024, INV>(st, a.out, w.off, w.lines, tw); break;
+            case 11: do_lines<2048, INV>(st, a.out, w.off, w.lines, tw); break;
+            default: do_lines<4096, INV>(st, a.out, w.off, w.lines, tw); break;
+        }
+        return;
+    }
+    const int l1 = w.logn / 2, l2 = w.logn - l1;
+    float2* mid = a.scratch + w.scratch;
+    if (w.kind == FSQ_COLS) {
+        const float2* tw = a.tabs.line_tw[l1 - 6];
+        const float2* fine = a.tabs.fine[w.logn - 13];
+        const float2* coarse = a.tabs.coarse[w.logn - 13];
+        const int col0 = w.index << (ilog2c(FSQ_POINTS) - l1);
+        switch (l1) {
+            case 6: do_cols<64, INV>(st, mid, l2, col0, tw, fine, coarse); break;
+            case 7: do_cols<128, INV>(st, mid, l2, col0, tw, fine, coarse); break;
+            case 8: do_cols<256, INV>(st, mid, l2, col0, tw, fine, coarse); break;
+            case 9: do_cols<512, INV>(st, mid, l2, col0, tw, fine, coarse); break;
+            default: do_cols<1024, INV>(st, mid, l2, col0, tw, fine, coarse); break;
+        }
+    } else {
+        const float2* tw = a.tabs.line_tw[l2 - 6];
+        const int row0 = w.index << (ilog2c(FSQ_POINTS) - l2);
+        const float2* rows = mid + ((long long)row0 << l2);
+        float2* dst = a.out + w.off;
+        const float scale = 1.0f / (float)(1LL << w.logn);
+        switch (l2) {
+            case 7: do_rows<128, INV>(st, rows, dst, l1, row0, tw, scale); break;
+            case 8: do_rows<256, INV>(st, rows, dst, l1, row0, tw, scale); break;
+            case 9: do_rows<512, INV>(st, rows, dst, l1, row0, tw, scale); break;
+            default: do_rows<1024, INV>(st, rows, dst, l1, row0, tw, scale); break;
+        }
+    }
+}
+
+// Item p runs on CTA p mod gridDim.x; while one item is transformed in one
+// stage buffer, the CTA's next item is copied into the other.
+template <bool INV>
+__global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM) k_fsq(const FsqArgs a) {
+    extern __shared__ __align__(128) float2 smem[];
+    const uint64_t pol = policy_evict_first();
+    int p = blockIdx.x;
+    if (p >= a.nitems) return;
+    issue(a, get_work(a, p), smem, pol);
+    cp_async_commit();
+    int s = 0;
+    for (; p < a.nitems; p += gridDim.x) {
+        const int q = p + gridDim.x;
+        if (q < a.nitems) issue(a, get_work(a, q), smem + (s ^ 1) * QSTAGE, pol);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();  // this item's copies have landed for every thread
+        compute<INV>(a, get_work(a, p), smem + s * QSTAGE);
+        __syncthreads();  // the stage is free before the next item's copies target it
+        s ^= 1;
+    }
+    cp_async_wait<0>();
+}
+
+}  // namespace
+
+cudaError_t fsq_prepare() {
+    for (auto k : {k_fsq<false>, k_fsq<true>}) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, QSMEM);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t fsq_launch(const FsqArgs& a, bool inverse, int sms, cudaStream_t s) {
+    if (a.nitems <= 0) return cudaSuccess;
+    long long grid = (long long)sms * FSQ_CTAS_PER_SM;
+    if (grid > a.nitems) grid = a.nitems;
+    if (inverse) k_fsq<true><<<(unsigned)grid, FSQ_THREADS, QSMEM, s>>>(a);
+    else k_fsq<false><<<(unsigned)grid, FSQ_THREADS, QSMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace mfft

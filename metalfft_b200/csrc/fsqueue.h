@@ -1,0 +1,89 @@
+// fsqueue.h -- the persistent item kernel shared by the mixed-size batch
+// (multi.cu) and the four-step plans for n > 16384 (fourstep.cu).
+//
+// Every work item is 4096 complex points handled by one 256-thread CTA (three
+// CTAs per SM).  A launch walks its item list with a static schedule (item p
+// on CTA p mod grid) and copies the next item's data into the CTA's second
+// stage buffer with cp.async while the current item is transformed:
+//   LINES  4096/n whole lines of one size n <= 4096
+//   COLS   one column tile of a four-step transform n = n1*n2 (n >= 8192):
+//          4096/n1 adjacent columns x n1 rows -> column FFTs, times
+//          W_n^{col*k1}, into the transform's scratch area (row-major, like
+//          the input)
+//   ROWS   one row group of that transform: 4096/n2 rows of the scratch
+//          area -> row FFTs -> out[k2*n1 + k1] (the transpose folded into a
+//          16-byte tile store)
+// A four-step batch is two launches on one stream: pass 0 runs every COLS
+// (and LINES) item, pass 1 every ROWS item, so no item ever waits for
+// another inside a launch and no inter-CTA synchronisation exists.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace mfft {
+
+constexpr int FSQ_THREADS = 256;
+constexpr int FSQ_POINTS = 4096;
+constexpr int FSQ_CTAS_PER_SM = 3;
+
+enum : int { FSQ_LINES = 0, FSQ_COLS = 1, FSQ_ROWS = 2 };
+
+struct FsqItem {
+    int kind;
+    int logn;       // log2 of the line size (LINES) or of the transform size
+    int index;      // COLS: column tile, ROWS: row group
+    int xform;      // four-step transform id (COLS / ROWS)
+    long long off;  // LINES: element offset of the first line
+    int lines;      // LINES: lines in this item
+    int pad;
+};
+
+struct FsqXform {
+    long long off;      // element offset of the transform in in / out
+    long long scratch;  // element offset of its intermediate in the scratch buffer
+    int logn;
+    int pad;
+};
+
+struct FsqTables {
+    const float2* line_tw[7];  // line twiddle rows (E = 16) for n = 64 .. 4096
+    const float2* fine[8];     // W_n^m = fine[m % 1024] * coarse[m / 1024], n = 2^13 .. 2^20
+    const float2* coarse[8];
+};
+
+struct FsqArgs {
+    const float2* in;
+    float2* out;
+    float2* scratch;       // four-step intermediates
+    const FsqItem* items;  // explicit item list (mixed sizes), or nullptr: uniform pass below
+    const FsqXform* xf;
+    int nitems;
+    // uniform pass over `batch` contiguous four-step transforms of 2^u_logn
+    // points: u_kind FSQ_COLS (pass 0) or FSQ_ROWS (pass 1), u_per items each;
+    // transform j's intermediate is scratch + j * 2^u_logn
+    int u_kind, u_logn, u_per;
+    FsqTables tabs;
+};
+
+// n = 2^m (m >= 13) as n1 * n2 with n1 = 2^floor(m/2) <= n2.
+inline void fsq_split(int logn, int* n1, int* n2) {
+    *n1 = 1 << (logn / 2);
+    *n2 = 1 << (logn - logn / 2);
+}
+// COLS and ROWS items of one four-step transform of 2^logn points.
+inline int fsq_cols_items(int logn) {
+    int n1, n2;
+    fsq_split(logn, &n1, &n2);
+    return n2 / (FSQ_POINTS / n1);
+}
+inline int fsq_rows_items(int logn) {
+    int n1, n2;
+    fsq_split(logn, &n1, &n2);
+    return n1 / (FSQ_POINTS / n2);
+}
+
+cudaError_t fsq_prepare();
+// Launches one pass over a.nitems items on `s`.
+cudaError_t fsq_launch(const FsqArgs& a, bool inverse, int sms, cudaStream_t s);
+
+}  // namespace mfft

@@ -208,3 +208,43 @@ def test_captured_graph_matches_direct_exec(M):
         torch.cuda.synchronize()
         assert torch.equal(y, y_ref) and torch.equal(r, r_ref)
     assert O.rel_rms(y.cpu().numpy(), O.truth(x0.cpu().numpy())) < TOL
+
+
+@pytest.mark.parametrize("n,b", [(1 << 15, 1030), (1 << 20, 35)])
+def test_fourstep_batch_spans_scratch_chunks(M, n, b):
+    """A four-step batch larger than the plan's intermediate (2^25 points)
+    runs as several column/row pass pairs: lines on both sides of the chunk
+    boundary must match FP64, forward and inverse, and in place."""
+    import torch
+    x = O.normal_c64((b, n), seed=n + b)
+    f = M.MetalFFT(n)
+    xd = torch.from_numpy(x).cuda()
+    y = torch.empty_like(xd)
+    f.exec(xd, y, b, M.FORWARD)
+    torch.cuda.synchronize()
+    assert M.lib.mfft_context_check(M.shared_context()) == 0
+    chunk = (1 << 25) // n
+    rows = sorted({0, 1, chunk - 1, chunk, min(chunk + 1, b - 1), b - 1})
+    Y = y.cpu().numpy()
+    ref = O.truth(x[rows])
+    for i, j in enumerate(rows):
+        assert O.rel_rms(Y[j][None], ref[i][None]) < TOL_BIG, j
+    z = y.clone()
+    f.exec(z, z, b, M.INVERSE)  # in place
+    torch.cuda.synchronize()
+    assert O.rel_rms(z.cpu().numpy(), x.astype(np.complex128)) < TOL_BIG
+
+
+def test_misaligned_device_buffer_is_rejected(M):
+    """Device buffers must be 16-byte aligned; an 8-byte-aligned view is an
+    invalidArgument error raised before anything is launched."""
+    import torch
+    n = 1 << 16
+    f = M.MetalFFT(n)
+    base = torch.zeros(n + 1, dtype=torch.complex64, device="cuda")
+    view = base[1:]
+    assert view.data_ptr() % 16 == 8
+    out = torch.empty(n, dtype=torch.complex64, device="cuda")
+    with pytest.raises(M.FFTError) as e:
+        f.exec(view, out, 1, M.FORWARD)
+    assert e.value.case == "invalidArgument"
