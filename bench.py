@@ -276,7 +276,7 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
         assert M.lib.mfft_context_check(M.shared_context()) == 0
         ntr = sum(c for _, c in classes)
         gbs = mb.points * 16 / (ms / args.steps / 1e3) / 1e9
-        line.update({"metric": "mixed-size FFT batch in one persistent launch: points/s",
+        line.update({"metric": "mixed-size FFT batch on the persistent item kernel: points/s",
                      "value": mb.points * world * args.steps / (ms_max / 1e3), "unit": "points/s",
                      "ms_per_step": ms_max / args.steps, "transforms_per_step": ntr,
                      "config": {"workload": "sizes 2^6..2^14 + 2^20, counts U{1..512} seeded, <= 2^26 points",

@@ -124,6 +124,13 @@ MFFT_API int mfft_context_sm_count(const mfft_ctx* ctx);
  * calls check after every call; device-pointer calls are checked here). */
 MFFT_API int mfft_context_check(mfft_ctx* ctx);
 
+/* Self-test of the failure path (no reference counterpart): runs a kernel
+ * whose mbarrier wait can never complete.  The wait gives up after limit_ns
+ * (1e3 .. 1e9), records a timeout in the context's device error word and the
+ * kernel returns; the call reads and clears that word and returns
+ * MFFT_ERR_TIMEOUT.  The context stays usable afterwards. */
+MFFT_API int mfft_selftest_bounded_wait(mfft_ctx* ctx, int64_t limit_ns);
+
 /* ---- plans: MetalFFT.init(size:) (MetalFFT.swift:27-51) ---------------- */
 
 /* n: power of two in [64, 2^20].  The reference accepts 64..16384

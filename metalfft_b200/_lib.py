@@ -26,6 +26,7 @@ SIGNATURES = [
     ("mfft_context_destroy", c_int, [c_void_p]),
     ("mfft_context_sm_count", c_int, [c_void_p]),
     ("mfft_context_check", c_int, [c_void_p]),
+    ("mfft_selftest_bounded_wait", c_int, [c_void_p, c_int64]),
     ("mfft_plan_create", c_int, [c_void_p, c_int64, P(c_void_p)]),
     ("mfft_plan_destroy", c_int, [c_void_p]),
     ("mfft_plan_size", c_int64, [c_void_p]),

@@ -16,6 +16,7 @@
 #include <utility>
 
 #include "capi_internal.h"
+#include "tma.cuh"
 
 using namespace mfft;
 
@@ -391,4 +392,38 @@ extern "C" int mfft_exec_c2c(mfft_plan* plan, const void* in, void* out, int64_t
             return launch_c2c_device(plan, (const float2*)di, (float2*)dout, batch, direction, s);
         },
         true);
+}
+
+// ---------------------------------------------------------------------------
+// failure-path self-test
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// Waits, through the same bounded helper the pipelines use, on phase 0 of an
+// mbarrier that expects one arrival nobody makes; gives up after limit_ns and
+// records DEV_ERR_TMA_TIMEOUT in the context's error word.
+__global__ void k_selftest_wait(int* dev_err, unsigned long long limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mfft::mbar_init(&bar, 1);
+        mfft::fence_proxy_async_smem();
+    }
+    __syncthreads();
+    if (!mfft::mbar_wait(&bar, 0, limit_ns) && threadIdx.x == 0)
+        mfft::report_device_error(dev_err, mfft::DEV_ERR_TMA_TIMEOUT);
+}
+
+}  // namespace
+
+extern "C" int mfft_selftest_bounded_wait(mfft_ctx* ctx, int64_t limit_ns) {
+    if (!ctx) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "ctx is NULL");
+    if (limit_ns < 1000 || limit_ns > 1000000000LL)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, limit_ns, -1, "limit_ns must be in [1e3, 1e9]");
+    DeviceGuard g(ctx->device);
+    k_selftest_wait<<<1, 32, 0, ctx->stream>>>(ctx->dev_err, (unsigned long long)limit_ns);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_error(e, "self-test launch");
+    return check_device_error(ctx);
 }
