@@ -50,6 +50,15 @@ struct ConvGeom {
     static constexpr int SMEM_F2 = LINES * spad_size(FFT);
     static constexpr bool ACC_SMEM = SMEM_F2 * 8 + LINES * 2 * FFT * 4 <= 227 * 1024;
     static constexpr int SMEM_BYTES = SMEM_F2 * 8 + (ACC_SMEM ? LINES * 2 * FFT * 4 : 0);
+    // backward: block 0's dx spectrum waits in shared memory (not in
+    // registers) while block 1 is transformed, where it fits
+    static constexpr bool STASH = ACC_SMEM && SMEM_BYTES + LINES * FFT * 8 <= 227 * 1024;
+    static constexpr int SMEM_BYTES_BWD = SMEM_BYTES + (STASH ? LINES * FFT * 8 : 0);
+    // forward CTAs of <= 256 threads run two per SM at 128 registers a
+    // thread; the backward kernel needs more registers than that and keeps
+    // one CTA per SM (measured: fft 4096 forward 15 % faster at two, backward
+    // 24 % slower)
+    static constexpr int MINB_FWD = THREADS <= 256 ? 2 : 1;
 };
 
 template <bool WS>
@@ -61,7 +70,7 @@ __device__ __forceinline__ void cta_sync() {
 // Unit u (a walker) owns block pairs [p0, p1) of nout blocks (virtual blocks
 // past nx read zeros, so the last overlap is flushed by the same code).
 template <int FFT>
-__global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
+__global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, ConvGeom<FFT>::MINB_FWD)
     k_conv_fwd(const float* __restrict__ x, long long nx, float* __restrict__ y, long long ny,
                const float2* __restrict__ H, const float2* __restrict__ tw, int hop, long long npairs,
                long long pairs_per_unit, int warm_blocks, float* __restrict__ acc_g) {
@@ -167,6 +176,8 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
 
     // dh spectrum accumulator: bin k lives at D[k], owned by one thread
     float2* D = G::ACC_SMEM ? smem + G::SMEM_F2 + lf * FFT : part + unit * FFT;
+    // this thread's slots of the stash (same bins as D)
+    float2* stash = smem + G::SMEM_F2 + G::LINES * FFT + lf * FFT;
 #pragma unroll
     for (int m = 0; m < CONV_E; ++m) D[t + m * T] = make_float2(0.f, 0.f);
 
@@ -204,8 +215,13 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
                 const float2 Xk = make_float2(dZ.y, -dZ.x);
                 const float2 Sk = cmul(Gk, cconj(__ldg(H + k)));
                 D[k] = cadd(D[k], cmul(Gk, cconj(Xk)));
-                if (q == 0) S[m] = Sk;
-                else S[m] = cconj(make_float2(S[m].x - Sk.y, S[m].y + Sk.x));
+                if (q == 0) {
+                    if constexpr (G::STASH) stash[k] = Sk;
+                    else S[m] = Sk;
+                } else {
+                    const float2 S0 = G::STASH ? stash[k] : S[m];
+                    S[m] = cconj(make_float2(S0.x - Sk.y, S0.y + Sk.x));
+                }
             }
             line_sync<G::WS>();
         }
@@ -335,7 +351,7 @@ cudaError_t prep_line() {
     using G = ConvGeom<FFT>;
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(k_conv_fwd<FFT>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES))) return e;
-    if ((e = cudaFuncSetAttribute(k_conv_bwd<FFT>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES))) return e;
+    if ((e = cudaFuncSetAttribute(k_conv_bwd<FFT>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES_BWD))) return e;
     const int ls = spad_size(FFT) * 8;
     if ((e = cudaFuncSetAttribute(k_dh_finish<FFT>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls))) return e;
     if ((e = cudaFuncSetAttribute(k_corr<FFT>, cudaFuncAttributeMaxDynamicSharedMemorySize, ls))) return e;
@@ -348,9 +364,10 @@ void l_fwd(dim3 grid, int smem, cudaStream_t s, const float* x, long long nx, fl
     k_conv_fwd<FFT><<<grid, ConvGeom<FFT>::THREADS, smem, s>>>(x, nx, y, ny, H, tw, hop, npairs, ppu, warm, accg);
 }
 template <int FFT>
-void l_bwd(dim3 grid, int smem, cudaStream_t s, const float* x, long long nx, const float* g, long long ny,
+void l_bwd(dim3 grid, int, cudaStream_t s, const float* x, long long nx, const float* g, long long ny,
            const float2* H, const float2* tw, int hop, long long nblocks, long long bpu, float* dx, float2* part) {
-    k_conv_bwd<FFT><<<grid, ConvGeom<FFT>::THREADS, smem, s>>>(x, nx, g, ny, H, tw, hop, nblocks, bpu, dx, part);
+    k_conv_bwd<FFT><<<grid, ConvGeom<FFT>::THREADS, ConvGeom<FFT>::SMEM_BYTES_BWD, s>>>(x, nx, g, ny, H, tw, hop,
+                                                                                     nblocks, bpu, dx, part);
 }
 template <int FFT>
 void l_dh(cudaStream_t s, const float2* D, const float2* tw, int K, float* dh) {
