@@ -94,6 +94,7 @@ typedef struct mfft_conv mfft_conv;
 typedef struct mfft_corr mfft_corr;
 typedef struct mfft_analyzer mfft_analyzer;
 typedef struct mfft_multi mfft_multi;
+typedef struct mfft_spectral mfft_spectral;
 
 /* ---- errors ------------------------------------------------------------ */
 
@@ -265,6 +266,32 @@ MFFT_API int mfft_analyzer_destroy(mfft_analyzer* a);
  * (the precondition of FFTAnalyzer.swift:108). */
 MFFT_API int mfft_analyzer_analyze(mfft_analyzer* a, const float* samples, int64_t count,
                           int64_t offset, void* spectrum, int flags, void* stream);
+
+/* ---- STFT and power spectra (DSP/STFT.swift, DSP/PSD.swift) ------------ */
+
+/* Frames of fft_size samples (power of two 64..16384) every hop_size samples,
+ * each multiplied by the window before its FFT: the frame loop of
+ * STFT(fftSize:hopSize:window:sampleRate:) (STFT.swift:35-55, 79-107) and of
+ * PSD.welch / PSD.coherence (PSD.swift:18-134), run as one launch. */
+MFFT_API int mfft_spectral_create(mfft_ctx* ctx, int64_t fft_size, int64_t hop_size, int window_kind,
+                                  double kaiser_beta, mfft_spectral** out);
+MFFT_API int mfft_spectral_destroy(mfft_spectral* s);
+/* STFT.frameCount(for:) (STFT.swift:58-61): (n - fft) / hop + 1, 0 if n < fft. */
+MFFT_API int64_t mfft_stft_frame_count(const mfft_spectral* s, int64_t sample_count);
+/* STFT.analyze (STFT.swift:79-88): spectra = frames x fft_size complex bins
+ * (STFTFrame.complex), power = frames x fft_size |X|^2 (STFTFrame.magnitudes,
+ * which are squared magnitudes).  Either output may be NULL. */
+MFFT_API int mfft_stft_analyze(mfft_spectral* s, const float* signal, int64_t n, void* spectra, float* power,
+                               int flags, void* stream);
+/* PSD.welch (PSD.swift:18-58): psd[k] = sum over frames |X_k|^2 /
+ * (frames * sum(w^2) * sample_rate), fft_size values; zeros when no frame. */
+MFFT_API int mfft_psd_welch(mfft_spectral* s, const float* signal, int64_t n, double sample_rate, float* psd,
+                            int flags, void* stream);
+/* PSD.coherence (PSD.swift:71-134): over the frames of min(na, nb) samples,
+ * C[k] = |sum A conj(B)|^2 / (sum |A|^2 sum |B|^2), 0 where the denominator is
+ * not positive; fft_size values. */
+MFFT_API int mfft_psd_coherence(mfft_spectral* s, const float* a, int64_t na, const float* b, int64_t nb,
+                                float* coherence, int flags, void* stream);
 
 /* ---- SAR range-Doppler chain (src/radar/, src/fft_sar_fused*.metal) ----- */
 

@@ -16,6 +16,9 @@ Reference API (docs/MetalFFT.swiftinterface:12-266) and its mirror here:
   Correlator(fftSize:)             -> Correlator(fft_size) .cross(a, b) .auto(x)
   FFTAnalyzer(size:sampleRate:window:) -> FFTAnalyzer(size, sample_rate, window)
     .analyze(_:) / .analyze(_:offset:) -> AnalysisResult
+  STFT(fftSize:hopSize:window:sampleRate:) -> STFT(fft_size, hop_size, window, sample_rate)
+    .analyze(_:) / .spectrogram(_:) / frameCount(for:) -> STFTFrames / dB array / frame_count
+  PSD.welch / PSD.coherence        -> PSD.welch / PSD.coherence (one launch for all frames)
   FFTError                         -> FFTError (same cases, Python exception)
 
 Host arrays (numpy, lists) follow the Swift arrays' copy-in / copy-out
@@ -32,7 +35,7 @@ from . import _lib
 __all__ = [
     "FFTError", "MetalFFT", "MultiChannelFFT", "Convolver", "FusedConvolver", "Correlator",
     "FFTAnalyzer", "AnalysisResult", "WindowType", "MixedBatch", "SARParameters", "SARTarget",
-    "SARPipeline", "lib", "shared_context",
+    "SARPipeline", "STFT", "STFTFrames", "PSD", "SpectralEstimator", "to_decibels", "lib", "shared_context",
 ]
 
 lib = _lib.load()
@@ -275,3 +278,4 @@ class MultiChannelFFT:
 from ._dsp import (AnalysisResult, Convolver, Correlator, FFTAnalyzer, FusedConvolver,  # noqa: E402
                    MixedBatch, WindowType)
 from ._sar import SARParameters, SARPipeline, SARTarget  # noqa: E402
+from ._spectral import PSD, STFT, SpectralEstimator, STFTFrames, to_decibels  # noqa: E402

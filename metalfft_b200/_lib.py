@@ -59,6 +59,12 @@ SIGNATURES = [
     ("mfft_analyzer_create", c_int,
      [c_void_p, c_int64, c_double, c_int, c_double, P(c_void_p)]),
     ("mfft_analyzer_destroy", c_int, [c_void_p]),
+    ("mfft_spectral_create", c_int, [c_void_p, c_int64, c_int64, c_int, c_double, P(c_void_p)]),
+    ("mfft_spectral_destroy", c_int, [c_void_p]),
+    ("mfft_stft_frame_count", c_int64, [c_void_p, c_int64]),
+    ("mfft_stft_analyze", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int, c_void_p]),
+    ("mfft_psd_welch", c_int, [c_void_p, c_void_p, c_int64, c_double, c_void_p, c_int, c_void_p]),
+    ("mfft_psd_coherence", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int, c_void_p]),
     ("mfft_analyzer_analyze", c_int,
      [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int, c_void_p]),
     ("mfft_sar_default_params", c_int, [c_int64, c_int64, c_int64, c_double, c_void_p]),

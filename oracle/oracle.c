@@ -596,3 +596,80 @@ void mfo_window(int kind, int n, double beta, double* w) {
         }
     }
 }
+
+/* ---- STFT / Welch PSD / coherence (FP64) ---------------------------------
+ * STFT.analyze (Sources/MetalFFT/DSP/STFT.swift:79-88, frame() :97-107):
+ * frames at pos = 0, hop, 2 hop, ... while pos + fft <= n; frame f = FFT of
+ * w[i] * x[f*hop + i] with zero imaginary part, all fft bins.
+ * PSD.welch (DSP/PSD.swift:18-58): sum over frames of |X|^2 per bin, times
+ * 1 / (frames * sum(w^2) * sample_rate).
+ * PSD.coherence (DSP/PSD.swift:71-134): Sxx, Syy, Sxy = sum |A|^2, |B|^2,
+ * A conj(B) over the frames of min(na, nb) samples; C = |Sxy|^2 / (Sxx Syy),
+ * 0 where the denominator is not positive. */
+
+int64_t mfo_stft_frames(int64_t n, int fft, int hop) {
+    if (n < fft || hop <= 0) return 0;
+    return (n - fft) / hop + 1;
+}
+
+/* out: frames x fft complex128 */
+void mfo_stft(const double* x, int64_t n, int fft, int hop, const double* w, double* out) {
+    const int64_t frames = mfo_stft_frames(n, fft, hop);
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < frames; ++f) {
+        double* z = out + 2 * f * fft;
+        for (int i = 0; i < fft; ++i) {
+            z[2 * i] = w[i] * x[f * hop + i];
+            z[2 * i + 1] = 0.0;
+        }
+        mfo_fft_c128(z, z, fft, 1, -1, 1);
+    }
+}
+
+/* returns the frame count; out: fft values */
+int64_t mfo_welch(const double* x, int64_t n, int fft, int hop, const double* w, double sample_rate, double* out) {
+    const int64_t frames = mfo_stft_frames(n, fft, hop);
+    memset(out, 0, sizeof(double) * fft);
+    if (frames == 0) return 0;
+    double* spec = (double*)malloc(sizeof(double) * 2 * frames * fft);
+    mfo_stft(x, n, fft, hop, w, spec);
+    double wss = 0.0;
+    for (int i = 0; i < fft; ++i) wss += w[i] * w[i];
+    for (int64_t f = 0; f < frames; ++f)
+        for (int k = 0; k < fft; ++k) {
+            const double* z = spec + 2 * (f * fft + k);
+            out[k] += z[0] * z[0] + z[1] * z[1];
+        }
+    const double inv = 1.0 / ((double)frames * wss * sample_rate);
+    for (int k = 0; k < fft; ++k) out[k] *= inv;
+    free(spec);
+    return frames;
+}
+
+int64_t mfo_coherence(const double* a, int64_t na, const double* b, int64_t nb, int fft, int hop, const double* w,
+                      double* out) {
+    const int64_t n = na < nb ? na : nb;
+    const int64_t frames = mfo_stft_frames(n, fft, hop);
+    memset(out, 0, sizeof(double) * fft);
+    if (frames == 0) return 0;
+    double* sa = (double*)malloc(sizeof(double) * 2 * frames * fft);
+    double* sb = (double*)malloc(sizeof(double) * 2 * frames * fft);
+    mfo_stft(a, n, fft, hop, w, sa);
+    mfo_stft(b, n, fft, hop, w, sb);
+    for (int k = 0; k < fft; ++k) {
+        double sxx = 0, syy = 0, xr = 0, xi = 0;
+        for (int64_t f = 0; f < frames; ++f) {
+            const double* p = sa + 2 * (f * fft + k);
+            const double* q = sb + 2 * (f * fft + k);
+            sxx += p[0] * p[0] + p[1] * p[1];
+            syy += q[0] * q[0] + q[1] * q[1];
+            xr += p[0] * q[0] + p[1] * q[1];
+            xi += p[1] * q[0] - p[0] * q[1];
+        }
+        const double den = sxx * syy;
+        out[k] = den > 0.0 ? (xr * xr + xi * xi) / den : 0.0;
+    }
+    free(sa);
+    free(sb);
+    return frames;
+}

@@ -43,6 +43,10 @@ def load():
             "mfo_corr_f64": (None, [_dp, _i64, _dp, _i64, _int, _dp]),
             "mfo_ref_corr_f32": (None, [_fp, _i64, _fp, _i64, _int, _fp]),
             "mfo_window": (None, [_int, _int, _dbl, _dp]),
+            "mfo_stft_frames": (_i64, [_i64, _int, _int]),
+            "mfo_stft": (None, [_dp, _i64, _int, _int, _dp, _dp]),
+            "mfo_welch": (_i64, [_dp, _i64, _int, _int, _dp, _dbl, _dp]),
+            "mfo_coherence": (_i64, [_dp, _i64, _dp, _i64, _int, _int, _dp, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -160,6 +164,36 @@ def window(kind, n, beta=6.0):
     w = np.empty(n, np.float64)
     load().mfo_window(kind, n, beta, _d(w))
     return w
+
+
+def stft_frames(n, fft, hop):
+    return load().mfo_stft_frames(n, fft, hop)
+
+
+def stft64(x, fft, hop, w):
+    """FP64 STFT (frames x fft complex128) of real x with window w."""
+    x = np.ascontiguousarray(x, np.float64)
+    w = np.ascontiguousarray(w, np.float64)
+    out = np.empty((stft_frames(len(x), fft, hop), fft), np.complex128)
+    load().mfo_stft(_d(x), len(x), fft, hop, _d(w), _d(out))
+    return out
+
+
+def welch64(x, fft, hop, w, sample_rate):
+    x = np.ascontiguousarray(x, np.float64)
+    w = np.ascontiguousarray(w, np.float64)
+    out = np.empty(fft, np.float64)
+    load().mfo_welch(_d(x), len(x), fft, hop, _d(w), sample_rate, _d(out))
+    return out
+
+
+def coherence64(a, b, fft, hop, w):
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    w = np.ascontiguousarray(w, np.float64)
+    out = np.empty(fft, np.float64)
+    load().mfo_coherence(_d(a), len(a), _d(b), len(b), fft, hop, _d(w), _d(out))
+    return out
 
 
 # ---- seeded generators shared by tests, smoke and bench ---------------------

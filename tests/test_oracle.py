@@ -285,3 +285,46 @@ def test_windows():
     assert np.all(O.window(5, 16) == 1.0)
     k = O.window(4, 33, 6.0)
     assert abs(k[16] - 1.0) < 1e-12 and abs(k[0] - k[32]) < 1e-12
+
+
+# ---- STFT / Welch / coherence oracle (DSP/STFT.swift, DSP/PSD.swift) --------
+
+def test_stft_oracle_matches_per_frame_pocketfft():
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(3000)
+    for fft, hop, kind in [(256, 128, 0), (256, 100, 4), (64, 64, 5)]:
+        w = O.window(kind, fft)
+        S = O.stft64(x, fft, hop, w)
+        frames = (len(x) - fft) // hop + 1  # STFT.swift:58-61
+        assert S.shape == (frames, fft) == (O.stft_frames(len(x), fft, hop), fft)
+        ref = np.fft.fft(np.stack([w * x[f * hop:f * hop + fft] for f in range(frames)]), axis=1)
+        assert np.abs(S - ref).max() < 1e-11 * np.abs(ref).max()
+    assert O.stft_frames(100, 256, 64) == 0
+
+
+def test_welch_oracle_known_answers():
+    # PSD.swift:53-56 normalisation, and a tone at an exact bin of a
+    # rectangular window: all power in bins b and N-b, sum = A^2 N / (2 fs)
+    fft, hop, fs, b, amp = 256, 128, 1000.0, 19, 1.5
+    n = 256 * 20
+    t = np.arange(n)
+    x = amp * np.cos(2 * np.pi * b * t / fft)
+    w = O.window(5, fft)
+    P = O.welch64(x, fft, hop, w, fs)
+    assert np.argmax(P[:fft // 2]) == b
+    others = np.delete(P, [b, fft - b])
+    assert others.max() < 1e-20
+    assert abs(P[b] - (amp / 2) ** 2 * fft / fs) < 1e-9 * P[b]
+    # no frame: zeros
+    assert not O.welch64(x[:100], fft, hop, w, fs).any()
+
+
+def test_coherence_oracle_known_answers():
+    rng = np.random.default_rng(6)
+    x = rng.standard_normal(8192)
+    y = rng.standard_normal(8192)
+    w = O.window(0, 256)
+    assert np.allclose(O.coherence64(x, 3.0 * x, 256, 128, w), 1.0, atol=1e-12)
+    c = O.coherence64(x, y, 256, 128, w)
+    assert 0.0 <= c.min() and c.max() < 0.5 and c.mean() < 0.05  # independent noise, 63 frames
+    assert not O.coherence64(x[:100], y, 256, 128, w).any()
