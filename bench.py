@@ -10,7 +10,7 @@ headline `value` is the faster of those whose relative RMS error against an
 FP64 FFT of sampled lines is <= 3e-6.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tc4096 | c2c4096x256 | mixed | conv | sar]
+                    [--workload tc4096 | c2c4096x256 | mixed | conv | sar | stft | psd]
 
 --workload selects another configuration (one JSON line each):
   c2c4096x256  N=4096 x 256 lines U[-1,1), forward then inverse per step, over a
@@ -22,6 +22,10 @@ FP64 FFT of sampled lines is <= 3e-6.
   sar          FP16 SAR chain 4096 pulses x 8192 range (64 targets, 10 dB):
                range matched filter, corner turn, azimuth FFT and the phase
                adjoint of sum |I|^4, one CUDA graph per step
+  stft         STFT of 2^24 N(0,1) samples, fftSize 1024, hop 512, Hann:
+               every frame's complex spectrum and |X|^2, one launch per step
+  psd          Welch PSD of 2^26 N(0,1) samples, fftSize 4096, hop 2048,
+               Hann, one launch (+ a fixed-order reduction) per step
 
 Under torchrun each rank transforms its own 16384 lines (weak scaling, no
 collective on the data path); rank 0 prints one JSON line.
@@ -58,7 +62,7 @@ def parse():
     p.add_argument("--batch", type=int, default=BATCH)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv", "sar"])
+    p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv", "sar", "stft", "psd"])
     return p.parse_args()
 
 
@@ -285,6 +289,47 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
                                   "frac": gbs / peak, "peak_source": peak_src,
                                   "note": "16 B per point algorithmic; four-step lines move 32 B"},
                      "gpu_launches": args.steps, "clocks": clk})
+    elif args.workload in ("stft", "psd"):
+        if args.workload == "stft":
+            n, fft, hop = 1 << 24, 1024, 512
+        else:
+            n, fft, hop = 1 << 26, 4096, 2048
+        rng = np.random.default_rng(SEED + rank)
+        x = torch.from_numpy(rng.standard_normal(n, dtype=np.float32)).cuda()
+        est = M.STFT(fft, hop, None, 48000.0)
+        frames = est.frame_count(n)
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        P = lambda a: ctypes.c_void_p(a.data_ptr())  # noqa: E731
+        if args.workload == "stft":
+            spec = torch.empty((frames, fft), dtype=torch.complex64, device="cuda")
+            power = torch.empty((frames, fft), dtype=torch.float32, device="cuda")
+
+            def step(i):
+                M._check(M.lib.mfft_stft_analyze(est._h, P(x), n, P(spec), P(power), M.DEVICE, st))
+            algo = 4 * n + frames * fft * 12  # signal in; spectra (8 B) and |X|^2 (4 B) out per bin
+            metric = "STFT (complex spectra + |X|^2 of every frame): input samples/s"
+            launches = 1
+        else:
+            out = torch.empty(fft, dtype=torch.float32, device="cuda")
+
+            def step(i):
+                M._check(M.lib.mfft_psd_welch(est._h, P(x), n, 48000.0, P(out), M.DEVICE, st))
+            algo = 4 * n  # the signal once; the partial sums stay in L2
+            metric = "Welch PSD: input samples/s"
+            launches = 2
+        ms_max, ms, clk = timed(step, args.steps, args.warmup, barrier, dist, uuid)
+        gbs = algo / (ms / args.steps / 1e3) / 1e9
+        line.update({"metric": metric, "value": n * world * args.steps / (ms_max / 1e3), "unit": "samples/s",
+                     "ms_per_step": ms_max / args.steps,
+                     "config": {"workload": "%d N(0,1) samples seeded, fftSize %d, hop %d, Hann window, %d frames"
+                                            % (n, fft, hop, frames),
+                                "l2": "input %d MiB%s" % (n * 4 >> 20, ", output %d MiB" % (frames * fft * 12 >> 20)
+                                                           if args.workload == "stft" else "")},
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak, "peak_source": peak_src,
+                                  "note": "algorithmic bytes: the signal once (frames overlap: re-reads hit L2)"
+                                          + (" plus the spectra and powers written" if args.workload == "stft" else "")},
+                     "gpu_launches": launches * args.steps, "clocks": clk})
     elif args.workload == "sar":
         prm = M.SARParameters.default(4096, 8192, 1024, 512.0)
         sar = M.SARPipeline(prm)

@@ -36,6 +36,9 @@ struct SpGeom {
     static constexpr int THREADS = T * LINES;
     static constexpr bool WS = (T <= 32);
     static constexpr int XCH = LINES * spad_size(FFT);  // exchange area, float2
+    // accumulation kernels: up to three CTAs of <= 256 threads per SM (80
+    // registers at fft 4096, no spills)
+    static constexpr int MINB = THREADS <= 256 ? 3 : 1;
     // per-line accumulator planes: Welch 1 (power), coherence 4 (Sxx, Syy, Re, Im Sxy)
     template <int PLANES>
     static constexpr bool acc_smem() {
@@ -121,7 +124,7 @@ __global__ void __launch_bounds__(SpGeom<FFT>::THREADS)
 // [u*per, (u+1)*per); line = frame f of a (re) and of b (im); sums |A|^2,
 // |B|^2, Re and Im of A conj(B).  Sums land in part[u][plane][FFT].
 template <int FFT, bool COH>
-__global__ void __launch_bounds__(SpGeom<FFT>::THREADS)
+__global__ void __launch_bounds__(SpGeom<FFT>::THREADS, SpGeom<FFT>::MINB)
     k_spec_acc(const float* __restrict__ a, const float* __restrict__ b, long long frames, int hop,
                const float* __restrict__ win, const float2* __restrict__ tw, long long work, long long per,
                float* __restrict__ part) {
@@ -206,6 +209,7 @@ struct SpKernels {
     void (*stft)(dim3, cudaStream_t, const float*, long long, int, const float*, const float2*, float2*, float*);
     void (*acc)(bool, dim3, cudaStream_t, const float*, const float*, long long, int, const float*, const float2*,
                 long long, long long, float*);
+    int (*acc_ctas_per_sm)(bool);
 };
 
 template <int FFT>
@@ -236,9 +240,20 @@ void sp_acc(bool coh, dim3 grid, cudaStream_t s, const float* a, const float* b,
                                                                                      per, part);
 }
 
+template <int FFT>
+int sp_acc_occ(bool coh) {
+    using G = SpGeom<FFT>;
+    int occ = 0;
+    cudaError_t e = coh ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spec_acc<FFT, true>, G::THREADS,
+                                                                        G::template smem_bytes<4>())
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spec_acc<FFT, false>, G::THREADS,
+                                                                        G::template smem_bytes<1>());
+    return (e == cudaSuccess && occ > 0) ? occ : 1;
+}
+
 #define MFFT_SPK(F)                                                                                         \
     {F, SpGeom<F>::THREADS, SpGeom<F>::LINES, SpGeom<F>::XCH * 8, SpGeom<F>::template smem_bytes<1>(),     \
-     SpGeom<F>::template smem_bytes<4>(), &sp_prepare<F>, &sp_stft<F>, &sp_acc<F>}
+     SpGeom<F>::template smem_bytes<4>(), &sp_prepare<F>, &sp_stft<F>, &sp_acc<F>, &sp_acc_occ<F>}
 
 const SpKernels g_spk[] = {MFFT_SPK(64),   MFFT_SPK(128),  MFFT_SPK(256),  MFFT_SPK(512),  MFFT_SPK(1024),
                            MFFT_SPK(2048), MFFT_SPK(4096), MFFT_SPK(8192), MFFT_SPK(16384)};
@@ -264,6 +279,7 @@ struct mfft_spectral {
     double window_sumsq = 0;
     float* part = nullptr;    // walker sums
     long long part_floats = 0;
+    int occ_welch = 0, occ_coh = 0;  // resident CTAs per SM of the accumulation kernels
 };
 
 extern "C" int mfft_spectral_destroy(mfft_spectral* s) {
@@ -385,11 +401,13 @@ int stft_device(mfft_spectral* s, const float* x, long long frames, float2* spec
     return MFFT_SUCCESS;
 }
 
-// walkers over `work` items (pairs or frames): about two per SM slot
+// walkers over `work` items (pairs or frames): one CTA per resident slot
 int acc_device(mfft_spectral* s, bool coh, const float* a, const float* b, long long frames, long long work,
                float scale, float* out, cudaStream_t st) {
     const int lines = s->k->lines;
-    long long units = (long long)s->ctx->sms * 2 * lines;
+    int& occ = coh ? s->occ_coh : s->occ_welch;
+    if (!occ) occ = s->k->acc_ctas_per_sm(coh);
+    long long units = (long long)s->ctx->sms * occ * lines;
     if (units > work) units = work;
     if (units < 1) units = 1;
     const long long per = work > 0 ? (work + units - 1) / units : 0;
