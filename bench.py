@@ -10,7 +10,7 @@ headline `value` is the faster of those whose relative RMS error against an
 FP64 FFT of sampled lines is <= 3e-6.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tc4096 | c2c4096x256 | mixed | conv | sar | stft | psd]
+                    [--workload tc4096 | c2c4096x256 | mixed | conv | sar | sarfocus | stft | psd]
 
 --workload selects another configuration (one JSON line each):
   c2c4096x256  N=4096 x 256 lines U[-1,1), forward then inverse per step, over a
@@ -22,6 +22,9 @@ FP64 FFT of sampled lines is <= 3e-6.
   sar          FP16 SAR chain 4096 pulses x 8192 range (64 targets, 10 dB):
                range matched filter, corner turn, azimuth FFT and the phase
                adjoint of sum |I|^4, one CUDA graph per step
+  sarfocus     the same scene through the whole range-Doppler algorithm:
+               range compression, azimuth FFT, RCMC + azimuth matched filter,
+               inverse azimuth FFT (focused FP16 image), four launches per step
   stft         STFT of 2^24 N(0,1) samples, fftSize 1024, hop 512, Hann:
                every frame's complex spectrum and |X|^2, one launch per step
   psd          Welch PSD of 2^26 N(0,1) samples, fftSize 4096, hop 2048,
@@ -62,7 +65,7 @@ def parse():
     p.add_argument("--batch", type=int, default=BATCH)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv", "sar", "stft", "psd"])
+    p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv", "sar", "sarfocus", "stft", "psd"])
     return p.parse_args()
 
 
@@ -330,6 +333,35 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
                                   "note": "algorithmic bytes: the signal once (frames overlap: re-reads hit L2)"
                                           + (" plus the spectra and powers written" if args.workload == "stft" else "")},
                      "gpu_launches": launches * args.steps, "clocks": clk})
+    elif args.workload == "sarfocus":
+        prm = M.SARParameters.default(4096, 8192, 1024, 512.0)
+        sar = M.SARPipeline(prm)
+        raw = sar.simulate(workloads.sar_targets(prm, 64, seed=SEED + rank), 10.0, SEED + rank)
+        h, sc = sar.quantize(raw)
+        del raw
+        phi = torch.zeros(prm.pulses, dtype=torch.float32, device="cuda")
+        img, isc = sar.forward(h, sc, phi)
+        foc, fsc = sar.focus(img, isc)
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        P = lambda a: ctypes.c_void_p(a.data_ptr())  # noqa: E731
+
+        def step(i):
+            M._check(M.lib.mfft_sar_forward(sar._h, P(h), P(sc), P(phi), P(img), P(isc), st))
+            M._check(M.lib.mfft_sar_focus(sar._h, P(img), P(isc), P(foc), P(fsc), 0, st))
+        ms_max, ms, clk = timed(step, args.steps, args.warmup, barrier, dist, uuid)
+        ns = prm.pulses * prm.range_n
+        algo = ns * 32  # four passes, each FP16 in + out
+        gbs = algo / (ms / args.steps / 1e3) / 1e9
+        line.update({"metric": "FP16 SAR range-Doppler algorithm to a focused image: complex samples/s",
+                     "value": ns * world * args.steps / (ms_max / 1e3), "unit": "samples/s",
+                     "ms_per_step": ms_max / args.steps, "dtype": "fp16 storage, fp32 compute",
+                     "config": {"workload": "4096 pulses x 8192 range, chirp 1024 samples TBP 512, 64 seeded "
+                                            "targets, 10 dB SNR; range compression, azimuth FFT, RCMC + azimuth "
+                                            "matched filter, inverse azimuth FFT"},
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak, "peak_source": peak_src,
+                                  "note": "32 B per complex sample: four passes of FP16 in + out"},
+                     "gpu_launches": 4 * args.steps, "clocks": clk})
     elif args.workload == "sar":
         prm = M.SARParameters.default(4096, 8192, 1024, 512.0)
         sar = M.SARPipeline(prm)

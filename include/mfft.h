@@ -364,6 +364,16 @@ MFFT_API int mfft_sar_backward_phase(mfft_sar* sar, const void* raw_h, const flo
 MFFT_API int mfft_sar_step_graph(mfft_sar* sar, const void* raw_h, const float* pulse_scale, const float* phase,
                                  void* image_h, float* image_scale, float* dphi, double* loss, void* stream);
 
+/* Focused image from the range-Doppler image of mfft_sar_forward (device
+ * pointers, same layouts): per Doppler row, range cell migration correction
+ * with an 8-tap Hamming-windowed sinc and the azimuth matched filter, then the
+ * inverse azimuth FFT (rda_kernels.metal:103-240, rda_fused_pipeline.swift:
+ * 248-368).  reference_signs = 1 uses the reference's formulas as written
+ * (input read at r - shift, filter exp(-j phase)); 0 uses r + shift and
+ * exp(+j phase), which focus the reference's own echo model. */
+MFFT_API int mfft_sar_focus(mfft_sar* sar, const void* rd_h, const float* rd_scale, void* focused_h,
+                            float* focused_scale, int reference_signs, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -277,5 +277,5 @@ class MultiChannelFFT:
 
 from ._dsp import (AnalysisResult, Convolver, Correlator, FFTAnalyzer, FusedConvolver,  # noqa: E402
                    MixedBatch, WindowType)
-from ._sar import SARParameters, SARPipeline, SARTarget  # noqa: E402
+from ._sar import SARParameters, SARPipeline, SARTarget, expected_bins, point_target_metrics  # noqa: E402
 from ._spectral import PSD, STFT, SpectralEstimator, STFTFrames, to_decibels  # noqa: E402

@@ -78,6 +78,7 @@ SIGNATURES = [
     ("mfft_sar_backward_phase", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("mfft_sar_step_graph", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p]),
+    ("mfft_sar_focus", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
 ]
 
 _lib = None

@@ -92,6 +92,18 @@ class SARPipeline:
                                     _stream(raw_h)))
         return img, isc
 
+    def focus(self, image_h, image_scale, reference_signs=False):
+        """Focused image (FP16, one scale per range column) from the
+        range-Doppler image of forward(): RCMC, azimuth matched filter and
+        inverse azimuth FFT (rda_kernels.metal:103-240).  reference_signs
+        reproduces the reference's RCMC direction and filter sign."""
+        import torch
+        out = torch.empty_like(image_h)
+        osc = torch.empty(self.params.range_n, dtype=torch.float32, device=image_h.device)
+        _check(lib.mfft_sar_focus(self._h, _p(image_h), _p(image_scale), _p(out), _p(osc),
+                                  1 if reference_signs else 0, _stream(image_h)))
+        return out, osc
+
     def backward_phase(self, raw_h, pulse_scale, phase):
         import torch
         d = torch.empty(self.params.pulses, dtype=torch.float32, device=raw_h.device)
@@ -120,3 +132,79 @@ class SARPipeline:
         v = h.float()
         c = v[..., 0] + 1j * v[..., 1]
         return c * (scale[:, None] if axis_scale == 0 else scale[None, :])
+
+
+def expected_bins(params, target):
+    """(range bin, azimuth bin) where a point target focuses
+    (src/radar/sar_simulator.swift:118-119)."""
+    c = 299792458.0
+    tau0 = 2.0 * params.center_range / c - (params.range_n // 2) / params.sample_rate
+    rg = int((2.0 * target.range_m / c - tau0) * params.sample_rate)
+    az = int((target.azimuth_m / params.velocity + (params.pulses // 2) / params.prf) * params.prf)
+    return rg, az
+
+
+def point_target_metrics(power, expected_rg, expected_az, radius=20):
+    """RadarMetrics.measureTarget (src/radar/radar_metrics.swift:57-268) on a
+    |I|^2 image (azimuth x range): peak search, range / azimuth cuts through
+    the peak, PSLR and ISLR against a -20 dB mainlobe, -3 dB widths, and SNR
+    of the peak over the two 64 x 64 corners."""
+    import numpy as np
+    m = np.asarray(power, dtype=np.float64)
+    na, nr = m.shape
+    a0, a1 = max(0, expected_az - radius), min(na - 1, expected_az + radius)
+    r0, r1 = max(0, expected_rg - radius), min(nr - 1, expected_rg + radius)
+    win = m[a0:a1 + 1, r0:r1 + 1]
+    ia, ir = np.unravel_index(int(np.argmax(win)), win.shape)
+    pa, pr = a0 + int(ia), r0 + int(ir)
+    peak = m[pa, pr]
+
+    def cut_metrics(cut, pk):
+        n = len(cut)
+        pv = cut[pk]
+        if pv <= 0:
+            return 0.0, 0.0, float(n)
+        db = lambda v: 10 * np.log10(v / pv) if v > 0 else -100.0  # noqa: E731
+        left = pk
+        for i in range(pk - 1, -1, -1):
+            if db(cut[i]) < -20.0:
+                left = i + 1
+                break
+            if i == 0:
+                left = 0
+        right = pk
+        for i in range(pk + 1, n):
+            if db(cut[i]) < -20.0:
+                right = i - 1
+                break
+            if i == n - 1:
+                right = n - 1
+        main = float(cut[left:right + 1].sum())
+        half = min(n // 4, 200)
+        wl, wr = max(0, pk - half), min(n - 1, pk + half)
+        side = [cut[i] for i in range(wl, wr + 1) if i < left or i > right]
+        side_e = float(np.sum(side)) if side else 0.0
+        side_max = float(np.max(side)) if side else 0.0
+        pslr = 10 * np.log10(side_max / pv) if side_max > 0 else -60.0
+        islr = 10 * np.log10(side_e / main) if side_e > 0 and main > 0 else -60.0
+        thr = pv * 0.5
+        l3 = float(pk)
+        for i in range(pk, max(0, pk - half) - 1, -1):
+            if cut[i] < thr:
+                l3 = i + (thr - cut[i]) / (cut[i + 1] - cut[i]) if i + 1 < n and cut[i + 1] > thr else float(i)
+                break
+        r3 = float(pk)
+        for i in range(pk, min(n, pk + half)):
+            if cut[i] < thr:
+                r3 = i - (thr - cut[i]) / (cut[i - 1] - cut[i]) if i > 0 and cut[i - 1] > thr else float(i)
+                break
+        return pslr, islr, r3 - l3
+
+    pslr_r, islr_r, res_r = cut_metrics(m[pa, :], pr)
+    pslr_a, islr_a, res_a = cut_metrics(m[:, pr], pa)
+    cs = 64
+    noise = np.concatenate([m[:cs, :cs].ravel(), m[na - cs:, nr - cs:].ravel()]).mean()
+    snr = 10 * np.log10(peak / noise) if noise > 0 else 60.0
+    return {"range_bin": pr, "azimuth_bin": pa, "peak": float(peak), "pslr_range": pslr_r,
+            "pslr_azimuth": pslr_a, "islr_range": islr_r, "islr_azimuth": islr_a, "snr": snr,
+            "res3db_range": res_r, "res3db_azimuth": res_a}

@@ -221,7 +221,7 @@ struct AzGeom {
 
 // pass B: azimuth FFT of C range columns; IMAGE: write the FP16 image;
 // GRAD: per-tile partials of dL/dphi and of L = sum |I|^4
-template <int NA, bool IMAGE, bool GRAD>
+template <int NA, bool IMAGE, bool GRAD, bool INV = false>
 __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
     k_sar_azimuth(const __half2* __restrict__ rc, const float* __restrict__ rc_scale, long long nr,
                   const float2* __restrict__ tw, __half2* __restrict__ image, float* __restrict__ image_scale,
@@ -239,9 +239,15 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
         const int p = t + m * T;
         const float2 u = __half22float2(rc[(long long)p * nr + col]);
         const float s = __ldg(rc_scale + p);
-        v[m] = make_float2(u.x * s, u.y * s);
+        v[m] = make_float2(u.x * s, INV ? -u.y * s : u.y * s);
     }
     fft_regs<NA, SAR_E, false>(v, t, ColLine<C>{smem, c}, tw);  // v[m] = I[k = t + m*T][col]
+    if constexpr (INV) {
+        // inverse transform along azimuth: conj(FFT(conj(x))) / NA
+        const float sc = 1.0f / (float)NA;
+#pragma unroll
+        for (int m = 0; m < SAR_E; ++m) v[m] = make_float2(v[m].x * sc, -v[m].y * sc);
+    }
     if constexpr (IMAGE) {
         float mx = 0.f;
 #pragma unroll
@@ -318,6 +324,79 @@ __global__ void k_sar_reduce(const float* __restrict__ part, long long tiles, lo
     }
 }
 
+// Per Doppler row: RCMC taps and the azimuth matched filter's phase (cycles
+// alpha + beta * r), computed on the host in FP64.
+struct RcmcRow {
+    double alpha, beta;  // filter phase in cycles for range bin r
+    float w[8];          // interpolation taps j = -3 .. 4
+    int c0;              // input index of tap j for output r: r + c0 + j
+    int valid;           // |lambda f_a / 2v| < 0.95 (else the row is zero)
+    float sign;          // +1: exp(+j phase); -1: exp(-j phase)
+    int pad;
+};
+
+// focus pass 1: one Doppler row per CTA.  In: the range-Doppler image (FP16,
+// one scale per range column); out: RCMC'd and matched-filtered row (FP16,
+// one scale per row), the input layout of the inverse azimuth pass.
+template <int NR>
+__global__ void __launch_bounds__(NR / SAR_E) k_sar_rcmc(const __half2* __restrict__ rd, const float* __restrict__ rd_scale,
+                                                          const RcmcRow* __restrict__ rows, __half2* __restrict__ out,
+                                                          float* __restrict__ out_scale) {
+    constexpr int T = NR / SAR_E;
+    extern __shared__ __align__(16) float2 line[];
+    __shared__ float red[32];
+    const long long k = blockIdx.x;
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int m = 0; m < SAR_E; ++m) {
+        const int r = t + m * T;
+        const float2 u = __half22float2(rd[k * NR + r]);
+        const float sc = __ldg(rd_scale + r);
+        line[r] = make_float2(u.x * sc, u.y * sc);
+    }
+    __syncthreads();
+    const RcmcRow R = rows[k];
+    float2 v[SAR_E];
+    float mx = 0.f;
+#pragma unroll
+    for (int m = 0; m < SAR_E; ++m) {
+        const int r = t + m * T;
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int idx = r + R.c0 + j - 3;
+            if (idx >= 0 && idx < NR) {
+                const float2 x = line[idx];
+                acc.x = fmaf(x.x, R.w[j], acc.x);
+                acc.y = fmaf(x.y, R.w[j], acc.y);
+            }
+        }
+        float2 h = make_float2(0.f, 0.f);
+        if (R.valid) {
+            // phase in cycles in FP64, reduced to [0, 1) before the FP32 sincospi
+            const double cyc = fma((double)r, R.beta, R.alpha);
+            const float f = (float)(cyc - floor(cyc));
+            float sn, cs;
+            sincospif(2.0f * f, &sn, &cs);
+            h = make_float2(cs, R.sign * sn);
+        }
+        v[m] = cmul(acc, h);
+        mx = fmaxf(mx, fmaxf(fabsf(v[m].x), fabsf(v[m].y)));
+    }
+    const float s = block_scale(cta_max(mx, red));
+    const float inv = 1.f / s;
+#pragma unroll
+    for (int m = 0; m < SAR_E; ++m) out[k * NR + t + m * T] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
+    if (t == 0) out_scale[k] = s;
+}
+
+typedef void (*rcmc_fn)(int grid, cudaStream_t, const __half2*, const float*, const RcmcRow*, __half2*, float*);
+template <int NR>
+void l_rcmc(int grid, cudaStream_t s, const __half2* rd, const float* rds, const RcmcRow* rows, __half2* out,
+            float* outs) {
+    k_sar_rcmc<NR><<<grid, NR / SAR_E, NR * 8, s>>>(rd, rds, rows, out, outs);
+}
+
 typedef void (*range_fn)(int grid, cudaStream_t, const __half2*, const float*, const float*, const float2*,
                          const float2*, __half2*, float*);
 typedef void (*az_fn)(int grid, cudaStream_t, const __half2*, const float*, long long, const float2*, __half2*, float*,
@@ -328,15 +407,17 @@ void l_range(int grid, cudaStream_t s, const __half2* raw, const float* ps, cons
              const float2* tw, __half2* rc, float* rcs) {
     k_sar_range<NR><<<grid, NR / SAR_E, spad_size(NR) * 8, s>>>(raw, ps, ph, H, tw, rc, rcs);
 }
-template <int NA, bool IMAGE, bool GRAD>
+template <int NA, bool IMAGE, bool GRAD, bool INV = false>
 void l_az(int grid, cudaStream_t s, const __half2* rc, const float* rcs, long long nr, const float2* tw, __half2* img,
           float* imgs, float* dp, double* lp) {
-    k_sar_azimuth<NA, IMAGE, GRAD><<<grid, AzGeom<NA>::THREADS, NA * AzGeom<NA>::C * 8, s>>>(rc, rcs, nr, tw, img, imgs,
-                                                                                            dp, lp);
+    k_sar_azimuth<NA, IMAGE, GRAD, INV><<<grid, AzGeom<NA>::THREADS, NA * AzGeom<NA>::C * 8, s>>>(rc, rcs, nr, tw, img,
+                                                                                                 imgs, dp, lp);
 }
 template <int NR>
 cudaError_t prep_range() {
-    return cudaFuncSetAttribute(k_sar_range<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, spad_size(NR) * 8);
+    cudaError_t e = cudaFuncSetAttribute(k_sar_range<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, spad_size(NR) * 8);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_sar_rcmc<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, NR * 8);
 }
 template <int NA>
 cudaError_t prep_az() {
@@ -344,6 +425,8 @@ cudaError_t prep_az() {
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(k_sar_azimuth<NA, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
     if ((e = cudaFuncSetAttribute(k_sar_azimuth<NA, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+    if ((e = cudaFuncSetAttribute(k_sar_azimuth<NA, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)))
+        return e;
     return cudaFuncSetAttribute(k_sar_azimuth<NA, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
 }
 
@@ -351,16 +434,19 @@ struct RangeK {
     int n;
     range_fn f;
     cudaError_t (*prep)();
+    rcmc_fn rcmc;
 };
 struct AzK {
     int n, cols;
-    az_fn fwd, bwd, both;
+    az_fn fwd, bwd, both, inv;
     cudaError_t (*prep)();
 };
-const RangeK g_range[] = {{512, &l_range<512>, &prep_range<512>},       {1024, &l_range<1024>, &prep_range<1024>},
-                          {2048, &l_range<2048>, &prep_range<2048>},    {4096, &l_range<4096>, &prep_range<4096>},
-                          {8192, &l_range<8192>, &prep_range<8192>},    {16384, &l_range<16384>, &prep_range<16384>}};
-#define MFFT_AZ(N) {N, AzGeom<N>::C, &l_az<N, true, false>, &l_az<N, false, true>, &l_az<N, true, true>, &prep_az<N>}
+#define MFFT_RANGE(N) {N, &l_range<N>, &prep_range<N>, &l_rcmc<N>}
+const RangeK g_range[] = {MFFT_RANGE(512),  MFFT_RANGE(1024), MFFT_RANGE(2048),
+                          MFFT_RANGE(4096), MFFT_RANGE(8192), MFFT_RANGE(16384)};
+#define MFFT_AZ(N)                                                                                              \
+    {N, AzGeom<N>::C, &l_az<N, true, false>, &l_az<N, false, true>, &l_az<N, true, true>, &l_az<N, true, false, true>, \
+     &prep_az<N>}
 const AzK g_az[] = {MFFT_AZ(64), MFFT_AZ(128), MFFT_AZ(256), MFFT_AZ(512), MFFT_AZ(1024), MFFT_AZ(2048), MFFT_AZ(4096)};
 
 const BatchedKernel* e16(int n) {
@@ -391,6 +477,10 @@ struct mfft_sar {
     long long tiles = 0;
     cudaGraphExec_t graph = nullptr;
     const void* g_key[8] = {};
+    // focusing (allocated by the first mfft_sar_focus)
+    __half2* rd2 = nullptr;      // RCMC'd, matched-filtered rows, FP16
+    float* rd2_scale = nullptr;  // one scale per Doppler row
+    RcmcRow* rows[2] = {};       // per-row taps / filter: [0] focusing signs, [1] reference signs
 };
 
 static int check_params(const mfft_sar_params* p) {
@@ -497,6 +587,10 @@ extern "C" int mfft_sar_destroy(mfft_sar* s) {
     cudaFree(s->rc_scale);
     cudaFree(s->dphi_part);
     cudaFree(s->loss_part);
+    cudaFree(s->rd2);
+    cudaFree(s->rd2_scale);
+    cudaFree(s->rows[0]);
+    cudaFree(s->rows[1]);
     delete s;
     return MFFT_SUCCESS;
 }
@@ -641,4 +735,78 @@ extern "C" int mfft_sar_step_graph(mfft_sar* s, const void* raw_h, const float* 
     cudaError_t e = cudaGraphLaunch(s->graph, st);
     if (e != cudaSuccess) return cuda_error(e, "SAR graph launch");
     return MFFT_SUCCESS;
+}
+
+// Focusing of the range-Doppler image (rda_kernels.metal:103-240,
+// rda_fused_pipeline.swift:248-368): per Doppler row f_a, RCMC by
+// dR = R0 (1/sqrt(1 - (lambda f_a / 2v)^2) - 1) with an 8-tap Hamming-windowed
+// sinc, times the azimuth matched filter of phase 4 pi q R0(r) / lambda, then
+// the inverse azimuth FFT.  The reference reads its RCMC input at r - shift
+// and multiplies by exp(-j phase); with its own echo model exp(-j 4 pi R /
+// lambda) both move the target away from focus (in FP64: its RCMC lowers the
+// peak below no correction at all, its filter moves the peak off the target),
+// so the default here is r + shift and exp(+j phase); reference_signs = 1
+// reproduces the reference's formulas exactly.  The reference takes PRF = 1000
+// inside its RCMC kernel, which is its only PRF; the parameters' prf is used.
+static void sar_rows(const mfft_sar_params& p, bool reference, std::vector<RcmcRow>& rows) {
+    const long long na = p.pulses, nr = p.range_n;
+    const double lambda = C_LIGHT / p.carrier, rho = C_LIGHT / (2.0 * p.sample_rate);
+    rows.assign((size_t)na, RcmcRow{});
+    for (long long k = 0; k < na; ++k) {
+        RcmcRow& R = rows[(size_t)k];
+        const double fa = (double)(k < na / 2 ? k : k - na) / (double)na * p.prf;
+        const double ratio = lambda * fa / (2.0 * p.velocity);
+        R.valid = fabs(ratio) < 0.95;
+        const double q = R.valid ? sqrt(1.0 - ratio * ratio) : 1.0;
+        const double shift = R.valid ? p.center_range * (1.0 / q - 1.0) / rho : 0.0;
+        const double d = reference ? -shift : shift;
+        const double c0 = floor(d), frac = d - c0;
+        R.c0 = (int)c0;
+        for (int j = -3; j <= 4; ++j) {
+            const double x = frac - (double)j;
+            const double sv = fabs(x) < 1e-6 ? 1.0 : sin(PI_D * x) / (PI_D * x);
+            R.w[j + 3] = (float)(sv * (0.54 - 0.46 * cos(2.0 * PI_D * (double)(j + 3) / 7.0)));
+        }
+        // phase / (2 pi) = 2 q R0(r) / lambda, R0(r) = R0 + (r - nr/2) rho
+        R.alpha = 2.0 * q * (p.center_range - (double)(nr / 2) * rho) / lambda;
+        R.beta = 2.0 * q * rho / lambda;
+        R.sign = reference ? -1.f : 1.f;
+    }
+}
+
+extern "C" int mfft_sar_focus(mfft_sar* s, const void* rd_h, const float* rd_scale, void* focused_h,
+                              float* focused_scale, int reference_signs, void* stream) {
+    if (!s || !rd_h || !rd_scale || !focused_h || !focused_scale)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "NULL argument");
+    if (reference_signs != 0 && reference_signs != 1)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, reference_signs, -1, "reference_signs must be 0 or 1");
+    DeviceGuard gd(s->ctx->device);
+    const long long na = s->prm.pulses, nr = s->prm.range_n;
+    cudaError_t e = cudaSuccess;
+    if (!s->rd2) {
+        e = cudaMalloc(&s->rd2, sizeof(__half2) * na * nr);
+        if (e == cudaSuccess) e = cudaMalloc(&s->rd2_scale, sizeof(float) * na);
+        if (e != cudaSuccess) {
+            cudaFree(s->rd2);
+            s->rd2 = nullptr;
+            return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "SAR focus buffers: %s", cudaGetErrorString(e));
+        }
+    }
+    RcmcRow*& rows = s->rows[reference_signs];
+    if (!rows) {
+        std::vector<RcmcRow> h;
+        sar_rows(s->prm, reference_signs != 0, h);
+        e = cudaMalloc(&rows, sizeof(RcmcRow) * na);
+        if (e == cudaSuccess) e = cudaMemcpy(rows, h.data(), sizeof(RcmcRow) * na, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(rows);
+            rows = nullptr;
+            return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "SAR focus rows: %s", cudaGetErrorString(e));
+        }
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    s->rk->rcmc((int)na, st, (const __half2*)rd_h, rd_scale, rows, s->rd2, s->rd2_scale);
+    s->ak->inv((int)s->tiles, st, s->rd2, s->rd2_scale, nr, s->tw_a, (__half2*)focused_h, focused_scale, nullptr,
+               nullptr);
+    return sar_check_launch("SAR focus");
 }

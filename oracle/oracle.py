@@ -265,3 +265,15 @@ def sar_loss_grad(params, raw, chirp, phi):
     loss = L.mfo_sar_loss_grad(ctypes.byref(p), raw.ctypes.data_as(_dp), ch.ctypes.data_as(_dp),
                                ph.ctypes.data_as(_dp), d.ctypes.data_as(_dp))
     return loss, d
+
+
+def sar_focus(params, rd, reference_signs=False):
+    """FP64 focusing (RCMC + azimuth matched filter + azimuth inverse FFT) of
+    a range-Doppler image (pulses x range_n, Doppler-major)."""
+    L = load()
+    L.mfo_sar_focus.restype = None
+    p, _ = _sar_args(params, [])
+    rd = np.ascontiguousarray(rd, np.complex128)
+    out = np.empty_like(rd)
+    L.mfo_sar_focus(ctypes.byref(p), rd.ctypes.data_as(_dp), int(bool(reference_signs)), out.ctypes.data_as(_dp))
+    return out

@@ -17,7 +17,9 @@
  *   azimuth FFT                    rda_fused_pipeline.swift:224-242 (unscaled
  *     forward FFT along the pulse index for every range bin);
  * and, with no reference counterpart, the per-pulse phase e^{j phi_p}, the
- * sharpness loss L = sum |I|^4 and its analytic gradient dL/dphi.
+ * sharpness loss L = sum |I|^4 and its analytic gradient dL/dphi;
+ *   RCMC + azimuth matched filter  src/radar/rda_kernels.metal:103-240 with
+ *     the reference's signs or the focusing ones (mfo_sar_focus below).
  */
 #include <math.h>
 #include <stdint.h>
@@ -178,4 +180,72 @@ double mfo_sar_loss_grad(const mfo_sar_params* p, const double* raw, const doubl
     free(u);
     free(G);
     return L;
+}
+
+/* Focusing of the range-Doppler image (FP64): RCMC and the azimuth matched
+ * filter of the reference's RDA (src/radar/rda_kernels.metal:103-240,
+ * rda_fused_pipeline.swift:248-368), then the azimuth inverse FFT (1/na).
+ * Per Doppler row k (FFT order: f_a = k/na * prf below na/2, (k-na)/na * prf
+ * above): ratio = lambda f_a / (2 v); valid when |ratio| < 0.95;
+ * q = sqrt(1 - ratio^2); dR = R0 (1/q - 1) (0 when not valid), R0 = center
+ * range; shift = dR / rho, rho = c / (2 fs).  RCMC output r = sum over taps
+ * j = -3..4 of in[c0 + r + j] * sinc(frac - j) * (0.54 - 0.46 cos(2 pi (j+3)/7)),
+ * src = r + d, d = -shift (reference) or +shift, c0 = floor(d), frac = d - c0.
+ * Filter: phase = 4 pi q R0(r) / lambda, R0(r) = R0 + (r - nr/2) rho;
+ * H = exp(-j phase) (reference) or exp(+j phase); 0 when not valid.
+ * rd and out: na x nr complex128, Doppler / azimuth major. */
+void mfo_sar_focus(const mfo_sar_params* p, const double* rd, int reference_signs, double* out) {
+    const int64_t na = p->pulses, nr = p->range_n;
+    const double lambda = SAR_C / p->carrier, rho = SAR_C / (2.0 * p->sample_rate);
+    double* tmp = (double*)malloc(sizeof(double) * 2 * na * nr);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < na; ++k) {
+        const double fa = (double)(k < na / 2 ? k : k - na) / (double)na * p->prf;
+        const double ratio = lambda * fa / (2.0 * p->velocity);
+        const int valid = fabs(ratio) < 0.95;
+        const double q = valid ? sqrt(1.0 - ratio * ratio) : 1.0;
+        const double shift = valid ? p->center_range * (1.0 / q - 1.0) / rho : 0.0;
+        const double d = reference_signs ? -shift : shift;
+        const double c0 = floor(d), frac = d - c0;
+        double w[8];
+        for (int j = -3; j <= 4; ++j) {
+            const double x = frac - (double)j;
+            const double sv = fabs(x) < 1e-6 ? 1.0 : sin(SAR_PI * x) / (SAR_PI * x);
+            w[j + 3] = sv * (0.54 - 0.46 * cos(2.0 * SAR_PI * (double)(j + 3) / 7.0));
+        }
+        for (int64_t r = 0; r < nr; ++r) {
+            double ar = 0.0, ai = 0.0;
+            for (int j = -3; j <= 4; ++j) {
+                const int64_t idx = (int64_t)c0 + r + j;
+                if (idx < 0 || idx >= nr) continue;
+                ar += rd[2 * (k * nr + idx)] * w[j + 3];
+                ai += rd[2 * (k * nr + idx) + 1] * w[j + 3];
+            }
+            double hr = 0.0, hi = 0.0;
+            if (valid) {
+                const double ph = 4.0 * SAR_PI * q * (p->center_range + (double)(r - nr / 2) * rho) / lambda;
+                hr = cos(ph);
+                hi = reference_signs ? -sin(ph) : sin(ph);
+            }
+            tmp[2 * (k * nr + r)] = ar * hr - ai * hi;
+            tmp[2 * (k * nr + r) + 1] = ar * hi + ai * hr;
+        }
+    }
+    /* inverse FFT along azimuth for every range column, 1/na */
+    double* col = (double*)malloc(sizeof(double) * 2 * na * nr);
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < nr; ++r)
+        for (int64_t k = 0; k < na; ++k) {
+            col[2 * (r * na + k)] = tmp[2 * (k * nr + r)];
+            col[2 * (r * na + k) + 1] = tmp[2 * (k * nr + r) + 1];
+        }
+    mfo_fft_c128(col, col, na, nr, +1, 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < nr; ++r)
+        for (int64_t k = 0; k < na; ++k) {
+            out[2 * (k * nr + r)] = col[2 * (r * na + k)] / (double)na;
+            out[2 * (k * nr + r) + 1] = col[2 * (r * na + k) + 1] / (double)na;
+        }
+    free(tmp);
+    free(col);
 }
