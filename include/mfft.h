@@ -185,6 +185,15 @@ MFFT_API int mfft_exec_c2c(mfft_plan* plan, const void* in, void* out, int64_t b
 MFFT_API int mfft_exec_c2c_tc(mfft_plan* plan, const void* in, void* out, int64_t batch,
                      int direction, int variant, int flags, void* stream);
 
+/* Real-input transforms (no reference counterpart: the reference packs real
+ * data as complex with a zero imaginary part, Convolve.swift:47-53,
+ * FFTAnalyzer.swift:98-100).  n = the plan's size, a power of two 64..16384.
+ * r2c: batch lines of n floats -> batch lines of n/2 + 1 complex bins
+ * (X_0 .. X_{n/2}; the rest follow from X_{n-k} = conj X_k).  c2r: the
+ * inverse, scaled by 1/n.  Two real lines share one complex transform. */
+MFFT_API int mfft_exec_r2c(mfft_plan* plan, const float* in, void* out, int64_t batch, int flags, void* stream);
+MFFT_API int mfft_exec_c2r(mfft_plan* plan, const void* in, float* out, int64_t batch, int flags, void* stream);
+
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory (an external allocator owns the device, a real-time host reserves
  * memory once at start-up, a plug-in host forbids allocation): the four-step

@@ -161,6 +161,36 @@ class MetalFFT:
         _check(st)
         return out
 
+    def forward_real(self, x):
+        """Real input, n/2 + 1 complex bins per line (rfft): host arrays
+        ([batch,] n) or a CUDA float32 tensor."""
+        return self._real(x, True)
+
+    def inverse_real(self, X):
+        """n/2 + 1 bins per line -> n real samples (irfft, 1/n scaled)."""
+        return self._real(X, False)
+
+    def _real(self, x, forward):
+        n, h = self.size, self.size // 2 + 1
+        fn = lib.mfft_exec_r2c if forward else lib.mfft_exec_c2r
+        if _is_cuda_tensor(x):
+            import torch
+            x = x.contiguous()
+            batch = x.numel() // (n if forward else h)
+            shape = x.shape[:-1] + ((h,) if forward else (n,))
+            out = torch.empty(shape, dtype=torch.complex64 if forward else torch.float32, device=x.device)
+            _check(fn(self._plan, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()), batch, DEVICE,
+                      _stream_of(x)))
+            return out
+        a = np.ascontiguousarray(np.asarray(x, dtype=np.float32 if forward else np.complex64))
+        if a.shape[-1] != (n if forward else h):
+            _fail(6, "expected last dimension %d, got %d" % (n if forward else h, a.shape[-1]),
+                  n if forward else h, a.shape[-1])
+        batch = a.size // a.shape[-1]
+        out = np.empty(a.shape[:-1] + ((h,) if forward else (n,)), np.complex64 if forward else np.float32)
+        _check(fn(self._plan, a.ctypes.data, out.ctypes.data, batch, HOST, None))
+        return out
+
     def capture(self, calls):
         """One CUDA graph of device-tensor execs.  `calls` is a list of
         (inp, out, batch, direction) or (inp, out, batch, direction,

@@ -38,6 +38,8 @@ SIGNATURES = [
     ("mfft_exec_c2c", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),
     ("mfft_exec_c2c_tc", c_int,
      [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p]),
+    ("mfft_exec_r2c", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]),
+    ("mfft_exec_c2r", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]),
     ("mfft_fourstep_noalloc", c_int, [c_void_p, c_void_p, c_int64, c_int64, c_int, c_void_p]),
     ("mfft_multi_create", c_int, [c_void_p, c_void_p, c_int, P(c_void_p)]),
     ("mfft_multi_destroy", c_int, [c_void_p]),

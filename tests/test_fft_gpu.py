@@ -248,3 +248,37 @@ def test_misaligned_device_buffer_is_rejected(M):
     with pytest.raises(M.FFTError) as e:
         f.exec(view, out, 1, M.FORWARD)
     assert e.value.case == "invalidArgument"
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_real_input_fft_matches_fp64(M, n):
+    """forward_real: n/2 + 1 bins of the FFT of real lines (odd batch: the
+    last line has no partner); inverse_real recovers the lines."""
+    b = 7
+    x = np.random.default_rng(n).standard_normal((b, n)).astype(np.float32)
+    f = M.MetalFFT(n)
+    X = f.forward_real(x)
+    assert X.shape == (b, n // 2 + 1)
+    ref = O.truth(x.astype(np.complex64))[:, : n // 2 + 1]
+    assert O.rel_rms(X, ref) < TOL
+    xr = f.inverse_real(X)
+    assert xr.shape == (b, n)
+    assert float(np.linalg.norm(xr - x) / np.linalg.norm(x)) < TOL
+
+
+def test_real_input_fft_device_and_errors(M):
+    import torch
+    n = 4096
+    x = torch.randn(9, n, device="cuda")
+    f = M.MetalFFT(n)
+    X = f.forward_real(x)
+    assert X.is_cuda and X.shape == (9, n // 2 + 1)
+    assert np.array_equal(X.cpu().numpy(), f.forward_real(x.cpu().numpy()))
+    back = f.inverse_real(X)
+    assert float(torch.linalg.vector_norm(back - x) / torch.linalg.vector_norm(x)) < TOL
+    with pytest.raises(M.FFTError) as e:
+        M.MetalFFT(1 << 16).forward_real(np.zeros(1 << 16, np.float32))
+    assert e.value.case == "unsupportedFFTSize"
+    with pytest.raises(M.FFTError) as e:
+        f.forward_real(np.zeros(n - 1, np.float32))
+    assert e.value.case == "invalidInputSize"
