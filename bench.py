@@ -10,7 +10,7 @@ headline `value` is the faster of those whose relative RMS error against an
 FP64 FFT of sampled lines is <= 3e-6.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tc4096 | c2c4096x256 | mixed | conv | sar | sarfocus | stft | psd]
+                    [--workload tc4096 | c2c4096x256 | mixed | conv | sar | sarfocus | stft | psd | xspec]
 
 --workload selects another configuration (one JSON line each):
   c2c4096x256  N=4096 x 256 lines U[-1,1), forward then inverse per step, over a
@@ -29,6 +29,11 @@ FP64 FFT of sampled lines is <= 3e-6.
                every frame's complex spectrum and |X|^2, one launch per step
   psd          Welch PSD of 2^26 N(0,1) samples, fftSize 4096, hop 2048,
                Hann, one launch (+ a fixed-order reduction) per step
+  xspec        cross-spectral density matrix of 8 channels x 2^23 samples
+               (a shared N(0,1) component plus N(0,1) noise per channel),
+               fftSize 1024, hop 512, Hann: powers, 28 cross-spectra and the
+               reference's per-frame coherence; two launches per L2-sized
+               chunk of frames + one reduction per step
 
 Under torchrun each rank transforms its own 16384 lines (weak scaling, no
 collective on the data path); rank 0 prints one JSON line.
@@ -65,7 +70,8 @@ def parse():
     p.add_argument("--batch", type=int, default=BATCH)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv", "sar", "sarfocus", "stft", "psd"])
+    p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv", "sar", "sarfocus", "stft", "psd",
+                                                        "xspec"])
     return p.parse_args()
 
 
@@ -333,6 +339,41 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
                                   "note": "algorithmic bytes: the signal once (frames overlap: re-reads hit L2)"
                                           + (" plus the spectra and powers written" if args.workload == "stft" else "")},
                      "gpu_launches": launches * args.steps, "clocks": clk})
+    elif args.workload == "xspec":
+        C, n, fft, hop = 8, 1 << 23, 1024, 512
+        rng = np.random.default_rng(SEED + rank)
+        common = rng.standard_normal(n, dtype=np.float32)
+        xh = np.stack([common + rng.standard_normal(n, dtype=np.float32) for _ in range(C)])
+        x = torch.from_numpy(xh).cuda()
+        del xh, common
+        est = M.SpectralEstimator(fft, hop)
+        frames = est.frame_count(n)
+        pairs = C * (C - 1) // 2
+        power = torch.empty((C, fft), dtype=torch.float32, device="cuda")
+        cross = torch.empty((pairs, fft), dtype=torch.complex64, device="cuda")
+        coh = torch.empty((pairs, fft), dtype=torch.float32, device="cuda")
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        P = lambda a: ctypes.c_void_p(a.data_ptr())  # noqa: E731
+
+        def step(i):
+            M._check(M.lib.mfft_psd_cross_spectral(est._h, P(x), C, n, P(power), P(cross), P(coh), 0, M.DEVICE, st))
+        ms_max, ms, clk = timed(step, args.steps, args.warmup, barrier, dist, uuid)
+        algo = 4 * C * n  # every channel's samples once; chunk spectra and sums stay in L2
+        gbs = algo / (ms / args.steps / 1e3) / 1e9
+        chunk = max(2, ((32 << 20) // (C * (fft // 2 + 16) * 8)) & ~1)
+        chunks = -(-frames // chunk)
+        line.update({"metric": "multi-channel cross-spectral density (Welch): channel samples/s",
+                     "value": C * n * world * args.steps / (ms_max / 1e3), "unit": "samples/s",
+                     "ms_per_step": ms_max / args.steps,
+                     "config": {"workload": "%d channels x %d samples (shared N(0,1) + N(0,1) noise) seeded, "
+                                            "fftSize %d, hop %d, Hann, %d frames, %d pairs, per-frame coherence"
+                                            % (C, n, fft, hop, frames, pairs),
+                                "l2": "input %d MiB; %d chunks of %d frames" % (4 * C * n >> 20, chunks, chunk)},
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak, "peak_source": peak_src,
+                                  "note": "algorithmic bytes: the signals once; the per-bin pair products "
+                                          "(28 pairs x 3 sums per bin and frame) make it compute-heavy"},
+                     "gpu_launches": (2 * chunks + 1) * args.steps, "clocks": clk})
     elif args.workload == "sarfocus":
         prm = M.SARParameters.default(4096, 8192, 1024, 512.0)
         sar = M.SARPipeline(prm)

@@ -302,6 +302,27 @@ MFFT_API int mfft_psd_welch(mfft_spectral* s, const float* signal, int64_t n, do
 MFFT_API int mfft_psd_coherence(mfft_spectral* s, const float* a, int64_t na, const float* b, int64_t nb,
                                 float* coherence, int flags, void* stream);
 
+/* PSD.crossSpectral (Sources/MetalFFT/DSP/CrossSpectral.swift:56-152, per-bin
+ * kernel Resources/fft_cross_spectral.metal:29-63): `signals` holds `channels`
+ * (1..16) real signals of `length` samples each, one after the other.  Frames
+ * as in mfft_stft_analyze; per frame and bin p_c = |X_c|^2 and, for the pairs
+ * (0,1), (0,2), ..., (0,C-1), (1,2), ..., (C-2,C-1), S_ij = X_i conj(X_j);
+ * outputs are means over the frames, fft_size bins each:
+ *   power      channels x fft_size      mean p_c
+ *   cross      pairs x fft_size complex mean S_ij (NULL allowed for 1 channel)
+ *   coherence  pairs x fft_size         coherence_mode 0: mean over frames of
+ *              |S_ij|^2 / max(p_i p_j, 1e-30), the reference's formula (1
+ *              wherever both channels have power, whatever their relation);
+ *              coherence_mode 1: the Welch estimate |mean S_ij|^2 /
+ *              (mean p_i mean p_j), 0 where the denominator is not positive.
+ * No frames: all outputs zero.  The sample rate only labels bins in the
+ * reference and is not an argument.  Device calls keep chunk spectra and
+ * partial sums in the handle (grown on demand), so one handle serves one
+ * stream at a time. */
+MFFT_API int mfft_psd_cross_spectral(mfft_spectral* s, const float* signals, int64_t channels, int64_t length,
+                                     float* power, void* cross, float* coherence, int coherence_mode, int flags,
+                                     void* stream);
+
 /* ---- SAR range-Doppler chain (src/radar/, src/fft_sar_fused*.metal) ----- */
 
 /* SARParameters (src/radar/sar_simulator.swift:22-67) with the chirp given by

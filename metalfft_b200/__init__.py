@@ -19,6 +19,7 @@ Reference API (docs/MetalFFT.swiftinterface:12-266) and its mirror here:
   STFT(fftSize:hopSize:window:sampleRate:) -> STFT(fft_size, hop_size, window, sample_rate)
     .analyze(_:) / .spectrogram(_:) / frameCount(for:) -> STFTFrames / dB array / frame_count
   PSD.welch / PSD.coherence        -> PSD.welch / PSD.coherence (one launch for all frames)
+  PSD.crossSpectral(channels:...)  -> PSD.cross_spectral(channels, fft_size, hop_size, ...)
   FFTError                         -> FFTError (same cases, Python exception)
 
 Host arrays (numpy, lists) follow the Swift arrays' copy-in / copy-out
@@ -35,7 +36,8 @@ from . import _lib
 __all__ = [
     "FFTError", "MetalFFT", "MultiChannelFFT", "Convolver", "FusedConvolver", "Correlator",
     "FFTAnalyzer", "AnalysisResult", "WindowType", "MixedBatch", "SARParameters", "SARTarget",
-    "SARPipeline", "STFT", "STFTFrames", "PSD", "SpectralEstimator", "to_decibels", "lib", "shared_context",
+    "SARPipeline", "STFT", "STFTFrames", "PSD", "SpectralEstimator", "CrossSpectralResult",
+    "COHERENCE_PER_FRAME", "COHERENCE_WELCH", "to_decibels", "lib", "shared_context",
 ]
 
 lib = _lib.load()
@@ -308,4 +310,5 @@ class MultiChannelFFT:
 from ._dsp import (AnalysisResult, Convolver, Correlator, FFTAnalyzer, FusedConvolver,  # noqa: E402
                    MixedBatch, WindowType)
 from ._sar import SARParameters, SARPipeline, SARTarget, expected_bins, point_target_metrics  # noqa: E402
-from ._spectral import PSD, STFT, SpectralEstimator, STFTFrames, to_decibels  # noqa: E402
+from ._spectral import (COHERENCE_PER_FRAME, COHERENCE_WELCH, PSD, STFT, CrossSpectralResult,  # noqa: E402
+                        SpectralEstimator, STFTFrames, to_decibels)

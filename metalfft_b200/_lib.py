@@ -67,6 +67,8 @@ SIGNATURES = [
     ("mfft_stft_analyze", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int, c_void_p]),
     ("mfft_psd_welch", c_int, [c_void_p, c_void_p, c_int64, c_double, c_void_p, c_int, c_void_p]),
     ("mfft_psd_coherence", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int, c_void_p]),
+    ("mfft_psd_cross_spectral", c_int,
+     [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]),
     ("mfft_analyzer_analyze", c_int,
      [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int, c_void_p]),
     ("mfft_sar_default_params", c_int, [c_int64, c_int64, c_int64, c_double, c_void_p]),

@@ -18,6 +18,22 @@
 //    memory when it does not fit, coherence at 16384) owned by one thread per
 //    bin, are written per walker and summed over walkers in a fixed order,
 //    then normalised: deterministic, no atomics.
+//
+// PSD.crossSpectral (DSP/CrossSpectral.swift:56-152) also loops per frame:
+// a multi-channel FFT, a per-bin kernel for |X_c|^2, X_i conj(X_j) and the
+// per-frame coherence (Resources/fft_cross_spectral.metal:29-63), then CPU
+// sums.  Here the frames go through in chunks small enough for their spectra
+// to stay in L2:
+//  * k_xstft transforms frame pairs of every channel of the chunk (the same
+//    two-real-frames-per-line split) and keeps bins 0 .. n/2 only (real
+//    input: X_{n-k} = conj X_k);
+//  * k_xspec_acc owns a tile of bins and a slice of the chunk's frames; its
+//    warp groups split the upper-triangle channel pairs, with the pair sums in
+//    registers and the channel values of a few frames staged in shared memory
+//    by cp.async; the sums of each frame slice carry over from chunk to chunk
+//    in a fixed order;
+//  * k_xspec_finish sums the slices in FP64, divides by the frame count and
+//    mirrors bins n/2+1 .. n-1 from their conjugates.
 #include <vector>
 
 #include "capi_internal.h"
@@ -202,6 +218,226 @@ __global__ void k_spec_finish(const float* __restrict__ part, long long units, i
     }
 }
 
+// ---- cross-spectral -----------------------------------------------------
+
+// spectra of a chunk: X[(f * C + c) * hs + k], k = 0 .. n/2, hs = n/2 + 16
+// (rows stay 128-byte aligned)
+__host__ __device__ constexpr int xs_stride(int fft) { return fft / 2 + 16; }
+
+template <int FFT>
+__global__ void __launch_bounds__(SpGeom<FFT>::THREADS)
+    k_xstft(const float* __restrict__ x, long long len, int C, long long f0, long long nf, int hop,
+            const float* __restrict__ win, const float2* __restrict__ tw, float2* __restrict__ X) {
+    using G = SpGeom<FFT>;
+    constexpr int T = G::T, HS = xs_stride(FFT);
+    extern __shared__ __align__(16) float2 smem[];
+    const int lf = threadIdx.x / T, t = threadIdx.x % T;
+    const PadLine buf{smem + lf * spad_size(FFT)};
+    const long long pairs = (nf + 1) / 2;
+    const long long l = (long long)blockIdx.x * G::LINES + lf;
+    const bool line_ok = l < (long long)C * pairs;  // idle lines still take part in the syncs
+    const int c = line_ok ? (int)(l / pairs) : 0;
+    const long long p = line_ok ? l - (long long)c * pairs : 0;
+    float w[SP_E];
+#pragma unroll
+    for (int m = 0; m < SP_E; ++m) w[m] = __ldg(win + t + m * T);
+    float2 v[SP_E];
+    load_pair<FFT>(x + (long long)c * len + f0 * hop, line_ok ? nf : 0, hop, p, t, w, v);
+    fft_regs<FFT, SP_E, G::WS>(v, t, buf, tw);
+    const bool ok0 = line_ok && 2 * p < nf, ok1 = line_ok && 2 * p + 1 < nf;
+    float2* r0 = X + (2 * p * C + c) * HS;
+    float2* r1 = r0 + (long long)C * HS;
+    hermitian_split<FFT, G::WS>(v, t, buf, [&](int m, float2 A, float2 B) {
+        const int k = t + m * T;
+        if (k <= FFT / 2) {
+            if (ok0) r0[k] = A;
+            if (ok1) r1[k] = B;
+        }
+    });
+}
+
+// k_xspec_acc geometry: G warp groups split the pairs; KB = XS_THREADS / G
+// bins per CTA; up to XQ pairs and xs_pmax(G) channel powers per thread; XF
+// frames per stage, two stages in flight.
+constexpr int XS_THREADS = 512, XQ = 8, XF = 2, XS_MAX_CH = 16, XS_MAX_G = 16;
+constexpr int XS_MAX_PAIRS = XS_MAX_CH * (XS_MAX_CH - 1) / 2;
+// largest channel count with ceil(P / G) <= XQ, divided over G groups
+__host__ __device__ constexpr int xs_pmax(int g) { return g == 1 ? 4 : g == 2 ? 3 : g <= 8 ? 2 : 1; }
+// smallest G in {1, 2, 4, 8, 16} with ceil(P / G) <= XQ
+inline int xs_groups(int C) {
+    const int P = C * (C - 1) / 2;
+    for (int g = 1; g < XS_MAX_G; g *= 2)
+        if ((P + g - 1) / g <= XQ) return g;
+    return XS_MAX_G;
+}
+inline int xs_smem(int C, int g) { return 2 * XF * C * (XS_THREADS / g) * (int)sizeof(float2); }
+
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gsrc), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_xs() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1_xs() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+// 1/x within one unit in the last place (PTX rcp.approx.f32)
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// CTA (blockIdx.x = bin tile, blockIdx.y = frame slice s) of one chunk of nf
+// frames.  part[(s * planes + plane) * nbins + k], planes: C powers, then
+// Re and Im of the P cross sums (interleaved per pair), then P per-frame
+// coherence sums (only when COH).  first: store, else add.
+template <int G, bool COH>
+__global__ void __launch_bounds__(XS_THREADS, 2)
+    k_xspec_acc(const float2* __restrict__ X, int C, int nbins, long long nf, int per, int first,
+                float* __restrict__ part) {
+    constexpr int KB = XS_THREADS / G, PMAX = xs_pmax(G);
+    extern __shared__ __align__(16) float2 stage[];  // [2][XF][C][KB]
+    // byte offsets (channel i, channel j) of every pair inside a frame's
+    // [C][KB] block, upper-triangle order (row i holds C - 1 - i pairs)
+    __shared__ uint2 pair_off[XS_MAX_PAIRS];
+    const int g = threadIdx.x / KB, b = threadIdx.x % KB;
+    const int hs = xs_stride(2 * (nbins - 1));
+    const int k = blockIdx.x * KB + b;
+    const bool live = k < nbins;
+    const int P = C * (C - 1) / 2;
+    const int qper = (P + G - 1) / G;
+    const int q0 = min(P, g * qper), qn = min(P, q0 + qper) - q0;
+    if (threadIdx.x < P) {
+        int r = threadIdx.x, i = 0;
+        while (r >= C - 1 - i) r -= C - 1 - i++;
+        pair_off[threadIdx.x] = make_uint2(i * KB * 8u, (i + 1 + r) * KB * 8u);
+    }
+    const int pn = g < C ? (C - g + G - 1) / G : 0;
+    float pw[PMAX], cr[XQ], ci[XQ], ch[XQ];
+#pragma unroll
+    for (int r = 0; r < PMAX; ++r) pw[r] = 0.f;
+#pragma unroll
+    for (int q = 0; q < XQ; ++q) cr[q] = ci[q] = ch[q] = 0.f;
+
+    const long long fa = (long long)blockIdx.y * per;
+    const long long fb = min(nf, fa + per);
+    const int nst = fb > fa ? (int)((fb - fa + XF - 1) / XF) : 0;
+    const int elems = XF * C * KB;  // float2 per stage
+    const int tile0 = blockIdx.x * KB;
+    // 16-byte copies of bin pairs (KB, tile0 and nbins - 1 = n/2 are even, so a
+    // pair never crosses a row's n/2 + 16 entries)
+    auto issue = [&](int si) {
+        float2* dst = stage + (si & 1) * elems;
+        const long long fs = fa + (long long)si * XF;
+        for (int e = 2 * threadIdx.x; e < elems; e += 2 * XS_THREADS) {
+            const int fr = e / (C * KB), rem = e - fr * C * KB, c = rem / KB, bb = rem - c * KB;
+            const long long f = fs + fr;
+            const bool ok = f < fb;
+            const int kk = min(tile0 + bb, nbins - 1);
+            cp_async16(dst + e, ok ? X + (f * C + c) * hs + kk : X, ok);
+        }
+    };
+    if (nst > 0) issue(0);
+    cp_async_commit_xs();
+    __syncthreads();  // pair_off
+    for (int si = 0; si < nst; ++si) {
+        if (si + 1 < nst) issue(si + 1);
+        cp_async_commit_xs();
+        cp_async_wait1_xs();
+        __syncthreads();
+        if (live) {
+            const char* U0 = reinterpret_cast<const char*>(stage + (si & 1) * elems + b);
+#pragma unroll
+            for (int fr = 0; fr < XF; ++fr) {
+                const char* U = U0 + fr * C * KB * 8;
+#pragma unroll
+                for (int r = 0; r < PMAX; ++r)
+                    if (r < pn) {
+                        const float2 u = *reinterpret_cast<const float2*>(U + (g + G * r) * KB * 8);
+                        pw[r] += u.x * u.x + u.y * u.y;
+                    }
+#pragma unroll
+                for (int q = 0; q < XQ; ++q)
+                    if (q < qn) {
+                        const uint2 o = pair_off[q0 + q];
+                        const float2 ui = *reinterpret_cast<const float2*>(U + o.x);
+                        const float2 uj = *reinterpret_cast<const float2*>(U + o.y);
+                        // S_ij = X_i conj(X_j) (fft_cross_spectral.metal:57-58)
+                        const float sr = ui.x * uj.x + ui.y * uj.y;
+                        const float sim = ui.y * uj.x - ui.x * uj.y;
+                        cr[q] += sr;
+                        ci[q] += sim;
+                        if constexpr (COH) {
+                            const float pi = ui.x * ui.x + ui.y * ui.y, pj = uj.x * uj.x + uj.y * uj.y;
+                            ch[q] += (sr * sr + sim * sim) * rcp_approx(fmaxf(pi * pj, 1e-30f));
+                        }
+                    }
+            }
+        }
+        __syncthreads();
+    }
+    if (!live) return;
+    const int planes = C + (COH ? 3 : 2) * P;
+    float* dst = part + (long long)blockIdx.y * planes * nbins + k;  // tiles partition the bins
+    auto put = [&](int plane, float v) {
+        float* d = dst + (long long)plane * nbins;
+        *d = first ? v : *d + v;
+    };
+#pragma unroll
+    for (int r = 0; r < PMAX; ++r)
+        if (r < pn) put(g + G * r, pw[r]);
+#pragma unroll
+    for (int q = 0; q < XQ; ++q)
+        if (q < qn) {
+            put(C + 2 * (q0 + q), cr[q]);
+            put(C + 2 * (q0 + q) + 1, ci[q]);
+            if constexpr (COH) put(C + 2 * P + q0 + q, ch[q]);
+        }
+}
+
+// one thread per (bin k <= n/2, item): items 0 .. C-1 are powers, C .. C+P-1
+// pairs.  Fixed-order FP64 sums over the frame slices, / frames, mirrored to n - k.
+// COH: coherence = mean of the per-frame values; else the Welch estimate
+// |sum S_ij|^2 / (sum p_i sum p_j) (0 where the denominator is not positive).
+template <bool COH>
+__global__ void k_xspec_finish(const float* __restrict__ part, int slices, int C, int nbins, long long frames,
+                               float* __restrict__ power, float2* __restrict__ cross, float* __restrict__ coh) {
+    const int P = C * (C - 1) / 2;
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (long long)(C + P) * nbins) return;
+    const int item = (int)(id / nbins), k = (int)(id - (long long)item * nbins);
+    const int n = 2 * (nbins - 1);
+    const int planes = C + (COH ? 3 : 2) * P;
+    const double inv = 1.0 / (double)frames;
+    auto sum = [&](int plane) {
+        double s = 0.0;
+        for (int u = 0; u < slices; ++u) s += part[((long long)u * planes + plane) * nbins + k];
+        return s;
+    };
+    const int km = (n - k) & (n - 1);
+    if (item < C) {
+        const float v = (float)(sum(item) * inv);
+        power[(long long)item * n + k] = v;
+        if (km != k) power[(long long)item * n + km] = v;
+        return;
+    }
+    const int q = item - C;
+    const double sr = sum(C + 2 * q), si = sum(C + 2 * q + 1);
+    const float2 s = make_float2((float)(sr * inv), (float)(si * inv));
+    cross[(long long)q * n + k] = s;
+    if (km != k) cross[(long long)q * n + km] = make_float2(s.x, -s.y);
+    float c;
+    if constexpr (COH) {
+        c = (float)(sum(C + 2 * P + q) * inv);
+    } else {
+        int i = 0, r = q;
+        while (r >= C - 1 - i) r -= C - 1 - i++;
+        const int j = i + 1 + r;
+        const double den = sum(i) * sum(j);
+        c = den > 0.0 ? (float)((sr * sr + si * si) / den) : 0.f;
+    }
+    coh[(long long)q * n + k] = c;
+    if (km != k) coh[(long long)q * n + km] = c;
+}
+
 struct SpKernels {
     int fft, threads, lines;
     int smem_stft, smem_welch, smem_coh;
@@ -210,6 +446,8 @@ struct SpKernels {
     void (*acc)(bool, dim3, cudaStream_t, const float*, const float*, long long, int, const float*, const float2*,
                 long long, long long, float*);
     int (*acc_ctas_per_sm)(bool);
+    void (*xstft)(dim3, cudaStream_t, const float*, long long, int, long long, long long, int, const float*,
+                  const float2*, float2*);
 };
 
 template <int FFT>
@@ -220,8 +458,14 @@ cudaError_t sp_prepare() {
     if ((e = cudaFuncSetAttribute(k_spec_acc<FFT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   G::template smem_bytes<1>())))
         return e;
+    if ((e = cudaFuncSetAttribute(k_xstft<FFT>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::XCH * 8))) return e;
     return cudaFuncSetAttribute(k_spec_acc<FFT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 G::template smem_bytes<4>());
+}
+template <int FFT>
+void sp_xstft(dim3 grid, cudaStream_t s, const float* x, long long len, int C, long long f0, long long nf, int hop,
+              const float* w, const float2* tw, float2* X) {
+    k_xstft<FFT><<<grid, SpGeom<FFT>::THREADS, SpGeom<FFT>::XCH * 8, s>>>(x, len, C, f0, nf, hop, w, tw, X);
 }
 template <int FFT>
 void sp_stft(dim3 grid, cudaStream_t s, const float* x, long long frames, int hop, const float* w, const float2* tw,
@@ -253,7 +497,7 @@ int sp_acc_occ(bool coh) {
 
 #define MFFT_SPK(F)                                                                                         \
     {F, SpGeom<F>::THREADS, SpGeom<F>::LINES, SpGeom<F>::XCH * 8, SpGeom<F>::template smem_bytes<1>(),     \
-     SpGeom<F>::template smem_bytes<4>(), &sp_prepare<F>, &sp_stft<F>, &sp_acc<F>, &sp_acc_occ<F>}
+     SpGeom<F>::template smem_bytes<4>(), &sp_prepare<F>, &sp_stft<F>, &sp_acc<F>, &sp_acc_occ<F>, &sp_xstft<F>}
 
 const SpKernels g_spk[] = {MFFT_SPK(64),   MFFT_SPK(128),  MFFT_SPK(256),  MFFT_SPK(512),  MFFT_SPK(1024),
                            MFFT_SPK(2048), MFFT_SPK(4096), MFFT_SPK(8192), MFFT_SPK(16384)};
@@ -263,6 +507,45 @@ const SpKernels* find_spk(int fft) {
         if (k.fft == fft) return &k;
     return nullptr;
 }
+
+template <int G, bool COH>
+void xs_launch(dim3 grid, int smem, cudaStream_t s, const float2* X, int C, int nbins, long long nf, int per,
+               int first, float* part) {
+    k_xspec_acc<G, COH><<<grid, XS_THREADS, smem, s>>>(X, C, nbins, nf, per, first, part);
+}
+using XsFn = void (*)(dim3, int, cudaStream_t, const float2*, int, int, long long, int, int, float*);
+XsFn xs_fn(int g, bool coh) {
+    switch (g) {
+        case 1: return coh ? &xs_launch<1, true> : &xs_launch<1, false>;
+        case 2: return coh ? &xs_launch<2, true> : &xs_launch<2, false>;
+        case 4: return coh ? &xs_launch<4, true> : &xs_launch<4, false>;
+        case 8: return coh ? &xs_launch<8, true> : &xs_launch<8, false>;
+        default: return coh ? &xs_launch<16, true> : &xs_launch<16, false>;
+    }
+}
+// shared-memory opt-in on the current device, then the resident CTAs per SM
+// (0 when the opt-in fails)
+template <int G, bool COH>
+int xs_occ_of(int smem) {
+    if (cudaFuncSetAttribute(k_xspec_acc<G, COH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return 0;
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xspec_acc<G, COH>, XS_THREADS, smem);
+    return (e == cudaSuccess && occ > 0) ? occ : 1;
+}
+int xs_occ(int g, bool coh, int smem) {
+    switch (g) {
+        case 1: return coh ? xs_occ_of<1, true>(smem) : xs_occ_of<1, false>(smem);
+        case 2: return coh ? xs_occ_of<2, true>(smem) : xs_occ_of<2, false>(smem);
+        case 4: return coh ? xs_occ_of<4, true>(smem) : xs_occ_of<4, false>(smem);
+        case 8: return coh ? xs_occ_of<8, true>(smem) : xs_occ_of<8, false>(smem);
+        default: return coh ? xs_occ_of<16, true>(smem) : xs_occ_of<16, false>(smem);
+    }
+}
+
+// spectra of one chunk stay at most this large (L2 holds them until the
+// accumulation reads them back)
+constexpr long long XS_CHUNK_BYTES = 32ll << 20;
 
 }  // namespace
 
@@ -280,6 +563,10 @@ struct mfft_spectral {
     float* part = nullptr;    // walker sums
     long long part_floats = 0;
     int occ_welch = 0, occ_coh = 0;  // resident CTAs per SM of the accumulation kernels
+    float2* xs_spec = nullptr;        // cross-spectral: spectra of one chunk
+    long long xs_spec_elems = 0;
+    float* xs_part = nullptr;         // cross-spectral: sums per frame slice
+    long long xs_part_floats = 0;
 };
 
 extern "C" int mfft_spectral_destroy(mfft_spectral* s) {
@@ -287,6 +574,8 @@ extern "C" int mfft_spectral_destroy(mfft_spectral* s) {
     DeviceGuard g(s->ctx->device);
     cudaFree(s->window);
     cudaFree(s->part);
+    cudaFree(s->xs_spec);
+    cudaFree(s->xs_part);
     delete s;
     return MFFT_SUCCESS;
 }
@@ -515,5 +804,111 @@ extern "C" int mfft_psd_coherence(mfft_spectral* s, const float* a, int64_t na, 
         }
         return acc_device(s, true, (const float*)bufs[0].dev, (const float*)bufs[1].dev, frames, frames, 1.f,
                           (float*)bufs[2].dev, cs);
+    });
+}
+
+namespace {
+
+int grow(void** p, long long& have, long long need, size_t elem, const char* what) {
+    if (need <= have) return MFFT_SUCCESS;
+    cudaFree(*p);
+    *p = nullptr;
+    have = 0;
+    cudaError_t e = cudaMalloc(p, elem * (size_t)need);
+    if (e != cudaSuccess) return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "%s: %s", what, cudaGetErrorString(e));
+    have = need;
+    return MFFT_SUCCESS;
+}
+
+int xspec_device(mfft_spectral* s, const float* x, int C, long long len, float* power, float2* cross, float* coh,
+                 int mode, cudaStream_t st) {
+    const int fft = (int)s->fft, nbins = fft / 2 + 1, hs = xs_stride(fft);
+    const int P = C * (C - 1) / 2;
+    const long long frames = mfft_stft_frame_count(s, len);
+    cudaError_t e;
+    if (frames == 0) {  // CrossSpectral.swift:130-133: zero accumulators
+        e = cudaMemsetAsync(power, 0, sizeof(float) * C * fft, st);
+        if (e == cudaSuccess && P) e = cudaMemsetAsync(cross, 0, sizeof(float2) * P * fft, st);
+        if (e == cudaSuccess && P) e = cudaMemsetAsync(coh, 0, sizeof(float) * P * fft, st);
+        return e == cudaSuccess ? MFFT_SUCCESS : cuda_error(e, "cross-spectral zero fill");
+    }
+    const bool per_frame = mode == 0;
+    const int g = xs_groups(C), kb = XS_THREADS / g, smem = xs_smem(C, g);
+    if ((C + g - 1) / g > xs_pmax(g) || (P + g - 1) / g > XQ)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, C, -1, "channel split %d does not fit", g);
+    const int tiles = (nbins + kb - 1) / kb;
+    // frames per chunk: even, at most XS_CHUNK_BYTES of spectra, no more than needed
+    long long fch = XS_CHUNK_BYTES / ((long long)C * hs * 8);
+    fch = fch < 2 ? 2 : fch & ~1LL;
+    if (fch > frames + (frames & 1)) fch = frames + (frames & 1);
+    // frame slices: enough CTAs to fill the GPU once over the bin tiles
+    const int occ = xs_occ(g, per_frame, smem);
+    if (!occ) return cuda_error(cudaGetLastError(), "cross-spectral kernel attributes");
+    long long slices = ((long long)s->ctx->sms * occ + tiles - 1) / tiles;
+    const long long max_slices = (fch + XF - 1) / XF;
+    if (slices > max_slices) slices = max_slices;
+    if (slices < 1) slices = 1;
+    long long per = (fch + slices - 1) / slices;
+    per = (per + XF - 1) / XF * XF;
+    slices = (fch + per - 1) / per;
+    const int planes = C + (per_frame ? 3 : 2) * P;
+    int rc = grow((void**)&s->xs_spec, s->xs_spec_elems, fch * C * hs, sizeof(float2), "cross-spectral spectra");
+    if (!rc) rc = grow((void**)&s->xs_part, s->xs_part_floats, slices * planes * nbins, sizeof(float),
+                       "cross-spectral sums");
+    if (rc) return rc;
+    const XsFn acc = xs_fn(g, per_frame);
+    for (long long f0 = 0; f0 < frames; f0 += fch) {
+        const long long nf = frames - f0 < fch ? frames - f0 : fch;
+        const long long lines = (long long)C * ((nf + 1) / 2);
+        const long long ctas = (lines + s->k->lines - 1) / s->k->lines;
+        s->k->xstft(dim3((unsigned)ctas), st, x, len, C, f0, nf, (int)s->hop, s->window, s->tw, s->xs_spec);
+        acc(dim3((unsigned)tiles, (unsigned)slices), smem, st, s->xs_spec, C, nbins, nf, (int)per, f0 == 0,
+            s->xs_part);
+    }
+    const long long items = (long long)(C + P) * nbins;
+    if (per_frame)
+        k_xspec_finish<true><<<(unsigned)((items + 255) / 256), 256, 0, st>>>(s->xs_part, (int)slices, C, nbins,
+                                                                             frames, power, cross, coh);
+    else
+        k_xspec_finish<false><<<(unsigned)((items + 255) / 256), 256, 0, st>>>(s->xs_part, (int)slices, C, nbins,
+                                                                              frames, power, cross, coh);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? MFFT_SUCCESS : cuda_error(e, "cross-spectral launch");
+}
+
+}  // namespace
+
+extern "C" int mfft_psd_cross_spectral(mfft_spectral* s, const float* signals, int64_t channels, int64_t length,
+                                       float* power, void* cross, float* coherence, int coherence_mode, int flags,
+                                       void* stream) {
+    if (!s) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "spectral handle is NULL");
+    int st = check_flags(flags);
+    if (st) return st;
+    // CrossSpectral.swift:63-66: 1..16 channels of one length
+    if (channels < 1 || channels > XS_MAX_CH)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, channels, -1, "crossSpectral requires 1-16 channels, got %lld",
+                         (long long)channels);
+    if (length < 0) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, length, -1, "signal length must be >= 0");
+    if (coherence_mode != 0 && coherence_mode != 1)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, coherence_mode, -1, "unknown coherence mode %d", coherence_mode);
+    const int C = (int)channels, P = C * (C - 1) / 2;
+    if (!power || (P && (!cross || !coherence)))
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "NULL output");
+    const long long frames = mfft_stft_frame_count(s, length);
+    if (frames > 0 && !signals) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "NULL signal");
+    if (frames > 0 && (long long)C * length > (1LL << 40))
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, length, -1, "signals too long");
+    DeviceGuard g(s->ctx->device);
+    if (flags == MFFT_DEVICE_MEMORY)
+        return xspec_device(s, signals, C, length, power, (float2*)cross, coherence, coherence_mode,
+                            (cudaStream_t)stream);
+    const size_t fft = (size_t)s->fft;
+    std::vector<HostBuf> bufs = {{signals, nullptr, frames > 0 ? (size_t)C * length * 4 : 0, nullptr},
+                                 {nullptr, power, (size_t)C * fft * 4, nullptr},
+                                 {nullptr, cross, (size_t)P * fft * 8, nullptr},
+                                 {nullptr, coherence, (size_t)P * fft * 4, nullptr}};
+    return host_call(s->ctx, bufs, [&](cudaStream_t cs) {
+        return xspec_device(s, (const float*)bufs[0].dev, C, length, (float*)bufs[1].dev, (float2*)bufs[2].dev,
+                            (float*)bufs[3].dev, coherence_mode, cs);
     });
 }

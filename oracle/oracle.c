@@ -673,3 +673,57 @@ int64_t mfo_coherence(const double* a, int64_t na, const double* b, int64_t nb, 
     free(sb);
     return frames;
 }
+
+/* ---- PSD.crossSpectral (FP64) ----------------------------------------------
+ * Sources/MetalFFT/DSP/CrossSpectral.swift:56-152 with the per-bin kernel
+ * Resources/fft_cross_spectral.metal:29-63: every frame (pos + fft <= n,
+ * pos += hop) of each channel is windowed and transformed; per frame and bin
+ * the kernel forms p_c = |X_c|^2, S_ij = X_i conj(X_j) for the upper-triangle
+ * pairs (0,1), (0,2), ..., (C-2,C-1) and the per-frame coherence
+ * |S_ij|^2 / max(p_i p_j, 1e-30); the host sums the three over frames and
+ * divides by the frame count (CrossSpectral.swift:134-151).  No frames: all
+ * zeros.  x: channels x n; power: channels x fft; cross: pairs x fft
+ * complex128; coh: pairs x fft.  Returns the frame count. */
+int64_t mfo_cross_spectral(const double* x, int channels, int64_t n, int fft, int hop, const double* w,
+                           double* power, double* cross, double* coh) {
+    const int pairs = channels * (channels - 1) / 2;
+    const int64_t frames = mfo_stft_frames(n, fft, hop);
+    memset(power, 0, sizeof(double) * channels * fft);
+    if (pairs) {
+        memset(cross, 0, sizeof(double) * 2 * pairs * fft);
+        memset(coh, 0, sizeof(double) * pairs * fft);
+    }
+    if (frames == 0) return 0;
+    double* spec = (double*)malloc(sizeof(double) * 2 * frames * fft * channels);
+    for (int c = 0; c < channels; ++c) mfo_stft(x + c * n, n, fft, hop, w, spec + 2 * (int64_t)c * frames * fft);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < fft; ++k) {
+        for (int64_t f = 0; f < frames; ++f) {
+            int pr = 0;
+            for (int i = 0; i < channels; ++i) {
+                const double* u = spec + 2 * (((int64_t)i * frames + f) * fft + k);
+                const double pi = u[0] * u[0] + u[1] * u[1];
+                power[i * fft + k] += pi;
+                for (int j = i + 1; j < channels; ++j, ++pr) {
+                    const double* v = spec + 2 * (((int64_t)j * frames + f) * fft + k);
+                    const double pj = v[0] * v[0] + v[1] * v[1];
+                    const double sr = u[0] * v[0] + u[1] * v[1];
+                    const double si = u[1] * v[0] - u[0] * v[1];
+                    cross[2 * (pr * fft + k)] += sr;
+                    cross[2 * (pr * fft + k) + 1] += si;
+                    const double den = pi * pj > 1e-30 ? pi * pj : 1e-30;
+                    coh[pr * fft + k] += (sr * sr + si * si) / den;
+                }
+            }
+        }
+        const double inv = 1.0 / (double)frames;
+        for (int c = 0; c < channels; ++c) power[c * fft + k] *= inv;
+        for (int q = 0; q < pairs; ++q) {
+            cross[2 * (q * fft + k)] *= inv;
+            cross[2 * (q * fft + k) + 1] *= inv;
+            coh[q * fft + k] *= inv;
+        }
+    }
+    free(spec);
+    return frames;
+}

@@ -47,6 +47,7 @@ def load():
             "mfo_stft": (None, [_dp, _i64, _int, _int, _dp, _dp]),
             "mfo_welch": (_i64, [_dp, _i64, _int, _int, _dp, _dbl, _dp]),
             "mfo_coherence": (_i64, [_dp, _i64, _dp, _i64, _int, _int, _dp, _dp]),
+            "mfo_cross_spectral": (_i64, [_dp, _int, _i64, _int, _int, _dp, _dp, _dp, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -194,6 +195,20 @@ def coherence64(a, b, fft, hop, w):
     out = np.empty(fft, np.float64)
     load().mfo_coherence(_d(a), len(a), _d(b), len(b), fft, hop, _d(w), _d(out))
     return out
+
+
+def cross_spectral64(x, fft, hop, w):
+    """FP64 PSD.crossSpectral of channels x n real samples: (power C x fft,
+    cross P x fft complex128, per-frame-averaged coherence P x fft)."""
+    x = np.ascontiguousarray(x, np.float64)
+    w = np.ascontiguousarray(w, np.float64)
+    c, n = x.shape
+    p = c * (c - 1) // 2
+    power = np.empty((c, fft), np.float64)
+    cross = np.zeros((max(p, 1), fft), np.complex128)
+    coh = np.zeros((max(p, 1), fft), np.float64)
+    load().mfo_cross_spectral(_d(x), c, n, fft, hop, _d(w), _d(power), _d(cross), _d(coh))
+    return power, cross[:p], coh[:p]
 
 
 # ---- seeded generators shared by tests, smoke and bench ---------------------

@@ -328,3 +328,45 @@ def test_coherence_oracle_known_answers():
     c = O.coherence64(x, y, 256, 128, w)
     assert 0.0 <= c.min() and c.max() < 0.5 and c.mean() < 0.05  # independent noise, 63 frames
     assert not O.coherence64(x[:100], y, 256, 128, w).any()
+
+
+def test_cross_spectral_oracle_known_answers():
+    # CrossSpectral.swift:56-152 / fft_cross_spectral.metal:29-63 restated:
+    # power = mean |X_c|^2 (the Welch PSD without its normalisation), cross =
+    # mean X_i conj(X_j), coherence = mean of per-frame |S|^2 / (p_i p_j) = 1
+    # wherever both channels have power, whatever the channels are
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal((3, 4096))
+    fft, hop, fs = 256, 128, 1000.0
+    w = O.window(0, fft)
+    pw, cr, ch = O.cross_spectral64(x, fft, hop, w)
+    assert pw.shape == (3, fft) and cr.shape == (3, fft) and ch.shape == (3, fft)
+    wss = float(np.sum(w * w))
+    for c in range(3):
+        assert np.allclose(pw[c], O.welch64(x[c], fft, hop, w, fs) * wss * fs, rtol=1e-12)
+    S = [O.stft64(x[c], fft, hop, w) for c in range(3)]
+    for q, (i, j) in enumerate([(0, 1), (0, 2), (1, 2)]):
+        assert np.allclose(cr[q], np.mean(S[i] * np.conj(S[j]), axis=0), rtol=1e-12, atol=1e-9)
+    assert np.allclose(ch, 1.0, atol=1e-12)
+    # the Welch estimate from these averages is PSD.coherence
+    assert np.allclose(np.abs(cr[0]) ** 2 / (pw[0] * pw[1]), O.coherence64(x[0], x[1], fft, hop, w), atol=1e-12)
+    # zero channels: per-frame 0 / max(0, 1e-30) = 0; too short: all zeros
+    z = O.cross_spectral64(np.zeros((2, 1024)), fft, hop, w)
+    assert not z[0].any() and not z[1].any() and not z[2].any()
+    s = O.cross_spectral64(x[:, :100], fft, hop, w)
+    assert not s[0].any() and not s[2].any()
+    one = O.cross_spectral64(x[:1], fft, hop, w)
+    assert one[1].shape == (0, fft) and one[2].shape == (0, fft)
+
+
+def test_cross_spectral_pair_index():
+    # CrossSpectral.swift:29-37 and CrossSpectralTests.swift:102-118
+    from metalfft_b200 import CrossSpectralResult
+    r = CrossSpectralResult(4, 1024, None, None, None)
+    assert [r.pair_index(i, j) for i, j in [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)]] == list(range(6))
+    assert r.pair_count == 6
+    r16 = CrossSpectralResult(16, 64, None, None, None)
+    flat = [(i, j) for i in range(16) for j in range(i + 1, 16)]
+    assert [r16.pair_index(i, j) for i, j in flat] == list(range(120))
+    with pytest.raises(ValueError):
+        r.pair_index(2, 1)
