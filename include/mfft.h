@@ -78,6 +78,15 @@ enum {
     MFFT_TC_BF16 = 2         /* plain BF16 operands, FP32 accumulate          */
 };
 
+/* FusedConvolver.Precision (Sources/MetalFFT/DSP/FusedConvolver.swift:27-36)
+ * for mfft_conv_set_precision. */
+enum {
+    MFFT_CONV_FLOAT32 = 0,      /* .float32 (default)                          */
+    MFFT_CONV_FP16_PURE = 1,    /* .float16Pure: all butterfly arithmetic FP16 */
+    MFFT_CONV_FP16_STORAGE = 2, /* .float16Storage: FP16 storage, FP32 math    */
+    MFFT_CONV_FP16_MIXED = 3    /* .float16Mixed: FP16 multiplies, FP32 adds   */
+};
+
 /* Window kinds (Sources/MetalFFT/DSP/Window.swift:6-24, WindowType). */
 enum {
     MFFT_WINDOW_HANN = 0,
@@ -240,6 +249,14 @@ MFFT_API int mfft_conv_destroy(mfft_conv* conv);
 MFFT_API int64_t mfft_conv_block_size(const mfft_conv* conv); /* Convolver.blockSize */
 MFFT_API int64_t mfft_conv_hop_size(const mfft_conv* conv);   /* Convolver.hopSize   */
 MFFT_API int64_t mfft_conv_kernel_len(const mfft_conv* conv);
+/* FusedConvolver(kernel:fftSize:precision:) (FusedConvolver.swift:55-83):
+ * the arithmetic of later mfft_conv_apply calls, one of MFFT_CONV_*.  The
+ * FP16 modes exist for fft_size 4096 only (FusedConvolver.supportedSize,
+ * :19); they store X and X*H as half2 and run the FFT exchanges through
+ * half2 shared memory, with the inverse's 1/N split as 2^-6 on H and 2^6/N
+ * at the end (exact power-of-two scalings that keep every FP16 value 64x
+ * below overflow).  mfft_conv_backward stays FP32 in every mode. */
+MFFT_API int mfft_conv_set_precision(mfft_conv* conv, int precision);
 /* Convolver.apply(to:) / FusedConvolver.apply(to:): out has n + kernel_len - 1
  * samples (Convolve.swift:36-76).  n == 0 gives kernel_len - 1 zeros. */
 MFFT_API int mfft_conv_apply(mfft_conv* conv, const float* signal, int64_t n, float* out, int flags,

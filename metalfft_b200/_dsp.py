@@ -100,17 +100,21 @@ class Convolver:
 
 class FusedConvolver(Convolver):
     """FusedConvolver (FusedConvolver.swift:17-134): the reference's single
-    dispatch FFT * H IFFT per block, fixed to fftSize 4096 and FP32 here."""
+    dispatch FFT * H IFFT per block, fftSize 4096, with its Precision modes
+    (:27-36) by their Swift case names: "float32" (default), "float16Pure",
+    "float16Storage", "float16Mixed"."""
 
     supported_size = 4096
+    PRECISIONS = {"float32": 0, "float16Pure": 1, "float16Storage": 2, "float16Mixed": 3}
 
     def __init__(self, kernel, fft_size=4096, precision="float32", context=None):
         if fft_size != self.supported_size:
             _fail(10, "FusedConvolver only supports fftSize=%d" % self.supported_size)
-        if precision != "float32":
-            _fail(10, "FusedConvolver precision %r is not built; float32 only" % (precision,))
-        self.precision = precision
+        if precision not in self.PRECISIONS:
+            _fail(10, "unknown FusedConvolver precision %r (one of %s)" % (precision, ", ".join(self.PRECISIONS)))
         super().__init__(kernel, fft_size, context)
+        _check(lib.mfft_conv_set_precision(self._h, self.PRECISIONS[precision]))
+        self.precision = precision
 
 
 class Correlator:

@@ -49,6 +49,7 @@ SIGNATURES = [
     ("mfft_conv_destroy", c_int, [c_void_p]),
     ("mfft_conv_block_size", c_int64, [c_void_p]),
     ("mfft_conv_hop_size", c_int64, [c_void_p]),
+    ("mfft_conv_set_precision", c_int, [c_void_p, c_int]),
     ("mfft_conv_kernel_len", c_int64, [c_void_p]),
     ("mfft_conv_apply", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int, c_void_p]),
     ("mfft_conv_backward", c_int,

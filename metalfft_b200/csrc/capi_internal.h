@@ -85,6 +85,14 @@ int check_device_error(mfft_ctx* ctx);
 int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, size_t out_bytes,
                     const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body, bool in_place = false);
 
+// FusedConvolver FP16 forward kernels (fft 4096, conv_fp16.cu): resident
+// CTAs per SM of a mode (0 if its attributes cannot be set), and the launch
+// with the FP32 forward kernel's walker arguments.
+int conv_fp16_ctas_per_sm(int mode);
+cudaError_t conv_fp16_forward(int mode, long long ctas, cudaStream_t s, const float* x, long long nx, float* y,
+                              long long ny, const float2* H, const float2* tw, int hop, long long npairs,
+                              long long ppu, int warm);
+
 // Line twiddle rows (E = 16) of size n, cached in the context.
 int line_twiddles(mfft_ctx* ctx, int n, float2** out);
 // W_n^m tables (fine[1024] then coarse[n / 1024]) for a four-step size n,

@@ -425,12 +425,14 @@ struct mfft_conv {
     long long part_units = 0;
     float* accg = nullptr;   // forward overlap accumulators when not in smem
     long long accg_units = 0;
+    int precision = MFFT_CONV_FLOAT32;  // forward arithmetic (FusedConvolver.Precision)
+    int fp16_occ = 0;                   // resident CTAs per SM of the FP16 forward kernel
 };
 
-static int conv_units(mfft_conv* c, long long work, long long* per_unit, long long* units) {
+static int conv_units(mfft_conv* c, long long work, long long* per_unit, long long* units, int per_sm = 2) {
     // enough walkers to fill the GPU, a few block pairs each
     const long long lines = c->lk->lines;
-    long long want = (long long)c->ctx->sms * 2 * lines;
+    long long want = (long long)c->ctx->sms * per_sm * lines;
     if (want > work) want = work;
     if (want < 1) want = 1;
     *per_unit = (work + want - 1) / want;
@@ -509,14 +511,37 @@ extern "C" int64_t mfft_conv_block_size(const mfft_conv* c) { return c ? c->fft 
 extern "C" int64_t mfft_conv_hop_size(const mfft_conv* c) { return c ? c->hop : 0; }
 extern "C" int64_t mfft_conv_kernel_len(const mfft_conv* c) { return c ? c->K : 0; }
 
+extern "C" int mfft_conv_set_precision(mfft_conv* c, int precision) {
+    if (!c) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "convolver is NULL");
+    if (precision < MFFT_CONV_FLOAT32 || precision > MFFT_CONV_FP16_MIXED)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, precision, -1, "unknown precision %d", precision);
+    if (precision != MFFT_CONV_FLOAT32) {
+        if (c->fft != 4096)  // FusedConvolver.swift:19, 56-57
+            return set_error(MFFT_ERR_INVALID_ARGUMENT, 4096, c->fft, -1,
+                             "FusedConvolver only supports fftSize=4096 in FP16 modes, got %lld", (long long)c->fft);
+        DeviceGuard g(c->ctx->device);
+        const int occ = conv_fp16_ctas_per_sm(precision);
+        if (occ <= 0) return cuda_error(cudaGetLastError(), "FP16 convolver kernel attributes");
+        c->fp16_occ = occ;
+    }
+    c->precision = precision;
+    return MFFT_SUCCESS;
+}
+
 static int conv_fwd_device(mfft_conv* c, const float* x, long long nx, float* y, cudaStream_t s) {
     const long long ny = nx + c->K - 1;
     const long long nout = (ny + c->hop - 1) / c->hop;  // output blocks (virtual zeros past nx)
     const long long npairs = (nout + 1) / 2;
     long long ppu, units;
+    const int warm = (int)((c->fft - 1) / c->hop);  // earlier blocks overlapping a range start
+    if (c->precision != MFFT_CONV_FLOAT32) {  // one walker per CTA, as many as are resident
+        conv_units(c, npairs, &ppu, &units, c->fp16_occ);
+        cudaError_t e = conv_fp16_forward(c->precision, units, s, x, nx, y, ny, c->H, c->tw, (int)c->hop, npairs,
+                                          ppu, warm);
+        return e == cudaSuccess ? MFFT_SUCCESS : cuda_error(e, "FP16 convolver launch");
+    }
     conv_units(c, npairs, &ppu, &units);
     const long long ctas = (units + c->lk->lines - 1) / c->lk->lines;
-    const int warm = (int)((c->fft - 1) / c->hop);  // earlier blocks overlapping a range start
     if (!c->lk->acc_smem && ctas * c->lk->lines > c->accg_units) {
         cudaFree(c->accg);
         c->accg = nullptr;
