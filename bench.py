@@ -194,6 +194,95 @@ def cpu_baseline(seconds=12.0):
                       "restatement of the reference, OpenMP over lines" % (reps, sample, N)}
 
 
+def cpu_baseline_other(workload, seconds=8.0):
+    """The reference's CPU path for a non-default workload: the oracle's
+    restatement (FP32 Stockham / four-step / overlap-add where the reference
+    has them, the FP64 chain for SAR and the spectral estimators) on all host
+    cores over a bounded sample of the same workload, in the workload's unit."""
+    import numpy as np
+    from oracle import oracle as O
+    from metalfft_b200 import workloads
+    rng = np.random.default_rng(SEED)
+    if workload == "c2c4096x256":
+        x = O.uniform_c64((256, 4096), SEED)
+
+        def fn():
+            O.ref_fft(O.ref_fft(x), inverse=True)
+        units, unit = 512, "transforms/s"
+        what = "256 lines of N=4096, forward then inverse, FP32 radix-4 Stockham restatement"
+    elif workload == "mixed":
+        # every size class, lines capped at 2^18 points per class
+        sample = [(n, max(1, min(c, (1 << 18) // n))) for n, c in workloads.mixed_size_classes()]
+        xs = [O.normal_c64((c, n), SEED + i) for i, (n, c) in enumerate(sample)]
+
+        def fn():
+            for x in xs:
+                O.ref_fft(x)
+        units, unit = sum(n * c for n, c in sample), "points/s"
+        what = "every size class of the batch, <= 2^18 points each (%d points), FP32 Stockham / four-step " \
+               "restatement" % units
+    elif workload in ("conv", "fconv"):
+        fft, K = (8192, 4095) if workload == "conv" else (4096, 512)
+        nx = 1 << 20
+        x = rng.standard_normal(nx).astype(np.float32)
+        h = rng.standard_normal(K).astype(np.float32)
+
+        def fn():
+            O.ref_conv(x, h, fft)
+        units, unit = nx, "samples/s"
+        what = "2^20 samples, %d taps, fftSize %d: the reference's overlap-add (FP32 forward FFT, complex " \
+               "multiply, inverse, overlap-add) restated; forward only (the reference has no adjoint)" % (K, fft)
+    elif workload in ("sar", "sarfocus"):
+        import metalfft_b200 as M
+        prm = M.SARParameters.default(256, 8192, 1024, 512.0)
+        raw = O.sar_simulate(prm, workloads.sar_targets(prm, 8, seed=SEED), 10.0, SEED)
+        ch = prm.chirp_reference()
+        phi = np.zeros(prm.pulses)
+        if workload == "sar":
+            def fn():
+                O.sar_loss_grad(prm, raw, ch, phi)
+            what = "256 pulses x 8192 range: FP64 range matched filter, corner turn, azimuth FFT and the " \
+                   "phase adjoint (oracle chain)"
+        else:
+            rd = O.sar_image(prm, raw, ch, phi)
+
+            def fn():
+                O.sar_focus(prm, O.sar_image(prm, raw, ch, phi))
+            del rd
+            what = "256 pulses x 8192 range: FP64 range compression, azimuth FFT, RCMC + azimuth matched " \
+                   "filter, inverse azimuth FFT (oracle chain)"
+        units, unit = prm.pulses * prm.range_n, "samples/s"
+    elif workload in ("stft", "psd"):
+        fft, hop = (1024, 512) if workload == "stft" else (4096, 2048)
+        n = 1 << 20
+        x = rng.standard_normal(n)
+        w = O.window(0, fft)
+        fn = (lambda: O.stft64(x, fft, hop, w)) if workload == "stft" else (lambda: O.welch64(x, fft, hop, w, 48000.0))
+        units, unit = n, "samples/s"
+        what = "2^20 samples, fftSize %d, hop %d, Hann: FP64 per-frame restatement" % (fft, hop)
+    elif workload == "xspec":
+        n = 1 << 17
+        x = rng.standard_normal((8, n))
+        w = O.window(0, 1024)
+
+        def fn():
+            O.cross_spectral64(x, 1024, 512, w)
+        units, unit = 8 * n, "samples/s"
+        what = "8 channels x 2^17 samples, fftSize 1024, hop 512: FP64 per-frame restatement"
+    else:
+        return None
+    fn()
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        fn()
+        reps += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": reps * units / dt, "unit": unit, "cores": O.max_threads(), "kind": "port",
+            "sample": "%d x (%s)" % (reps, what)}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -248,7 +337,8 @@ def timed(fn, steps, warmup, barrier, dist, uuid):
 
 
 def run_other(args, M, rank, world, dist, barrier, uuid):
-    """config 1 (c2c4096x256), config 2 (mixed), config 4 (conv)."""
+    """Every workload but the default one (configs 1, 2, 4, 5 and the
+    spectral, SAR-focusing and FusedConvolver-precision workloads)."""
     import ctypes
 
     import numpy as np
@@ -504,6 +594,8 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
                                   "note": "algorithmic bytes: x, y read/written by forward; x, g read and dx "
                                           "written by backward (g = y - t by one torch kernel)"},
                      "gpu_launches": 4 * args.steps, "clocks": clk})
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_other(args.workload)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
