@@ -183,6 +183,19 @@ extern "C" int mfft_context_destroy(mfft_ctx* ctx) {
         return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "the shared context is never destroyed");
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->h2d) {
+        cudaStreamSynchronize(ctx->h2d);
+        cudaStreamSynchronize(ctx->d2h);
+        cudaStreamDestroy(ctx->h2d);
+        cudaStreamDestroy(ctx->d2h);
+        for (int i = 0; i < mfft::STAGE_SLOTS; ++i) {
+            cudaEventDestroy(ctx->ev_up[i]);
+            cudaEventDestroy(ctx->ev_done[i]);
+            cudaEventDestroy(ctx->ev_down[i]);
+        }
+        cudaFree(ctx->stage);
+    }
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     for (auto& kv : ctx->twiddles) cudaFree(kv.second);
     cudaFree(ctx->dev_err);
     cudaStreamDestroy(ctx->stream);
@@ -339,18 +352,42 @@ int check_device_error(mfft_ctx* ctx) {
 
 // Host-array call: stage through one device buffer on the context stream and
 // wait, like MetalFFT's copy-in / commitAndWait / copy-out.
+// the context's device pool: keeps what it has reserved between calls, so a
+// repeated host-array call does not map and unmap its buffers every time
+static int ctx_pool(mfft_ctx* ctx, cudaMemPool_t* out) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!ctx->pool) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = ctx->device;
+        cudaMemPool_t p = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&p, &props);
+        if (e != cudaSuccess) return cuda_error(e, "device memory pool");
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        ctx->pool = p;
+    }
+    *out = ctx->pool;
+    return MFFT_SUCCESS;
+}
+
 int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, size_t out_bytes,
                     const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body, bool in_place) {
     cudaStream_t s = ctx->stream;
     void* d_in = nullptr;
     void* d_out = nullptr;
-    cudaError_t e = cudaMallocAsync(&d_in, in_bytes ? in_bytes : 16, s);
+    cudaMemPool_t pool = nullptr;
+    int pst = ctx_pool(ctx, &pool);
+    if (pst) return pst;
+    cudaError_t e = cudaMallocFromPoolAsync(&d_in, in_bytes ? in_bytes : 16, pool, s);
     if (e != cudaSuccess) return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "Device buffer allocation failed: %s", cudaGetErrorString(e));
     const bool same = in_place && (in_bytes == out_bytes);
     if (same) {
         d_out = d_in;
     } else {
-        e = cudaMallocAsync(&d_out, out_bytes ? out_bytes : 16, s);
+        e = cudaMallocFromPoolAsync(&d_out, out_bytes ? out_bytes : 16, pool, s);
         if (e != cudaSuccess) {
             cudaFreeAsync(d_in, s);
             cudaStreamSynchronize(s);
@@ -373,6 +410,91 @@ int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, s
     return st;
 }
 
+static int stage_init(mfft_ctx* ctx) {
+    if (ctx->h2d) return MFFT_SUCCESS;
+    cudaError_t e = cudaMalloc(&ctx->stage, STAGE_SLOT_BYTES * 2 * STAGE_SLOTS);
+    if (e != cudaSuccess) {
+        ctx->stage = nullptr;
+        return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "staging slots: %s", cudaGetErrorString(e));
+    }
+    cudaStream_t a = nullptr, b = nullptr;
+    e = cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking);
+    for (int i = 0; i < STAGE_SLOTS && e == cudaSuccess; ++i) {
+        e = cudaEventCreateWithFlags(&ctx->ev_up[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_done[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_down[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        if (a) cudaStreamDestroy(a);
+        if (b) cudaStreamDestroy(b);
+        for (int i = 0; i < STAGE_SLOTS; ++i) {
+            if (ctx->ev_up[i]) cudaEventDestroy(ctx->ev_up[i]);
+            if (ctx->ev_done[i]) cudaEventDestroy(ctx->ev_done[i]);
+            if (ctx->ev_down[i]) cudaEventDestroy(ctx->ev_down[i]);
+            ctx->ev_up[i] = ctx->ev_done[i] = ctx->ev_down[i] = nullptr;
+        }
+        cudaFree(ctx->stage);
+        ctx->stage = nullptr;
+        return cuda_error(e, "staging streams");
+    }
+    ctx->h2d = a;
+    ctx->d2h = b;
+    return MFFT_SUCCESS;
+}
+
+int run_host_lines(mfft_ctx* ctx, const void* in, void* out, int64_t lines, size_t in_line, size_t out_line,
+                   const std::function<int(const void* d_in, void* d_out, int64_t lines, cudaStream_t)>& body,
+                   bool in_place, bool pair) {
+    const size_t line_max = in_line > out_line ? in_line : out_line;
+    int64_t per = line_max ? (int64_t)(STAGE_SLOT_BYTES / line_max) : lines;
+    if (pair) per &= ~(int64_t)1;
+    if (per < 1 || lines <= per)
+        return run_host_staged(
+            ctx, in, out, (size_t)lines * in_line, (size_t)lines * out_line,
+            [&](void* di, void* dout, cudaStream_t s) { return body(di, dout, lines, s); }, in_place);
+    std::lock_guard<std::mutex> lk(ctx->stage_mu);
+    int st = stage_init(ctx);
+    if (st) return st;
+    cudaStream_t sc = ctx->stream, sh = ctx->h2d, sd = ctx->d2h;
+    char* slot = (char*)ctx->stage;
+    cudaError_t e = cudaSuccess;
+    // uploads start after the compute stream's earlier work (the slots may
+    // still be read by the previous call's last transforms)
+    e = cudaEventRecord(ctx->ev_done[0], sc);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(sh, ctx->ev_done[0], 0);
+    const int64_t nch = (lines + per - 1) / per;
+    for (int64_t c = 0; c < nch && e == cudaSuccess && !st; ++c) {
+        const int k = (int)(c % STAGE_SLOTS);
+        const int64_t l0 = c * per, nl = lines - l0 < per ? lines - l0 : per;
+        char* din = slot + (size_t)k * 2 * STAGE_SLOT_BYTES;
+        char* dout = in_place ? din : din + STAGE_SLOT_BYTES;
+        // slot k is free once the download of chunk c - STAGE_SLOTS is done
+        if (c >= STAGE_SLOTS) e = cudaStreamWaitEvent(sh, ctx->ev_down[k], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(din, (const char*)in + (size_t)l0 * in_line, (size_t)nl * in_line,
+                                cudaMemcpyHostToDevice, sh);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_up[k], sh);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(sc, ctx->ev_up[k], 0);
+        if (e != cudaSuccess) break;
+        st = body(din, dout, nl, sc);
+        if (st) break;
+        e = cudaEventRecord(ctx->ev_done[k], sc);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(sd, ctx->ev_done[k], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync((char*)out + (size_t)l0 * out_line, dout, (size_t)nl * out_line,
+                                cudaMemcpyDeviceToHost, sd);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_down[k], sd);
+    }
+    if (!st && e != cudaSuccess) st = cuda_error(e, "staged copies");
+    cudaError_t e1 = cudaStreamSynchronize(sh), e2 = cudaStreamSynchronize(sc), e3 = cudaStreamSynchronize(sd);
+    if (!st && e1 != cudaSuccess) st = cuda_error(e1, "execution");
+    if (!st && e2 != cudaSuccess) st = cuda_error(e2, "execution");
+    if (!st && e3 != cudaSuccess) st = cuda_error(e3, "execution");
+    if (!st) st = check_device_error(ctx);
+    return st;
+}
+
 }  // namespace mfft
 
 extern "C" int mfft_exec_c2c(mfft_plan* plan, const void* in, void* out, int64_t batch, int direction,
@@ -385,11 +507,11 @@ extern "C" int mfft_exec_c2c(mfft_plan* plan, const void* in, void* out, int64_t
     if (flags == MFFT_DEVICE_MEMORY)
         return launch_c2c_device(plan, (const float2*)in, (float2*)out, batch, direction,
                                  (cudaStream_t)stream);
-    size_t bytes = (size_t)batch * (size_t)plan->n * sizeof(float2);
-    return run_host_staged(
-        plan->ctx, in, out, bytes, bytes,
-        [&](void* di, void* dout, cudaStream_t s) {
-            return launch_c2c_device(plan, (const float2*)di, (float2*)dout, batch, direction, s);
+    const size_t line = (size_t)plan->n * sizeof(float2);
+    return run_host_lines(
+        plan->ctx, in, out, batch, line, line,
+        [&](const void* di, void* dout, int64_t nl, cudaStream_t s) {
+            return launch_c2c_device(plan, (const float2*)di, (float2*)dout, nl, direction, s);
         },
         true);
 }

@@ -24,6 +24,14 @@ struct mfft_ctx {
     std::mutex mu;
     std::map<std::pair<int, int>, float2*> twiddles;     // (n, e) -> twiddle rows
     std::map<int, const mfft::BatchedKernel*> tuned;     // n -> autotuned kernel
+    // host-array calls: a memory pool that keeps its memory between calls,
+    // and the chunked pipeline of line-independent transforms (upload and
+    // download streams, staging slots, one event ring per stage)
+    cudaMemPool_t pool = nullptr;
+    std::mutex stage_mu;
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    void* stage = nullptr;
+    cudaEvent_t ev_up[4] = {}, ev_done[4] = {}, ev_down[4] = {};
 };
 
 namespace mfft {
@@ -82,6 +90,17 @@ int launch_c2c_device(mfft_plan* plan, const float2* in, float2* out, int64_t ba
 int check_device_error(mfft_ctx* ctx);
 // Host-array call: copy in, run `body` on device buffers, copy out, wait.
 // in_place: the kernels may read and write one buffer (batched FFTs).
+// Host arrays of `lines` independent lines (in_line / out_line bytes each):
+// chunks of <= STAGE_SLOT_BYTES are uploaded on ctx->h2d, transformed in order
+// on ctx->stream by body(d_in, d_out, chunk_lines, stream) and downloaded on
+// ctx->d2h, so that the two copy directions and the transforms overlap;
+// `pair` keeps chunk boundaries on even lines.  Returns after the last
+// download.  Falls back to run_host_staged for one chunk.
+constexpr size_t STAGE_SLOT_BYTES = 16u << 20;
+constexpr int STAGE_SLOTS = 4;
+int run_host_lines(mfft_ctx* ctx, const void* in, void* out, int64_t lines, size_t in_line, size_t out_line,
+                   const std::function<int(const void* d_in, void* d_out, int64_t lines, cudaStream_t)>& body,
+                   bool in_place, bool pair = false);
 int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, size_t out_bytes,
                     const std::function<int(void* d_in, void* d_out, cudaStream_t)>& body, bool in_place = false);
 

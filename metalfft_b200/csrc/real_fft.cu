@@ -146,8 +146,8 @@ int real_exec(mfft_plan* plan, const void* in, void* out, int64_t batch, int fla
         return set_error(MFFT_ERR_UNSUPPORTED_SIZE, plan->n, -1, -1,
                          "real-input FFT sizes are powers of two 64..16384, got %lld", (long long)plan->n);
     if (batch == 0) return MFFT_SUCCESS;
-    const long long ctas = ((batch + 1) / 2 + k->lines - 1) / k->lines;
-    if (ctas > 0x7fffffffLL) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, batch, -1, "batch too large");
+    if (((batch + 1) / 2 + k->lines - 1) / k->lines > 0x7fffffffLL)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, batch, -1, "batch too large");
     DeviceGuard g(plan->ctx->device);
     cudaError_t e = k->prepare();  // shared-memory opt-in on the current device
     if (e != cudaSuccess) return cuda_error(e, "real FFT kernel attributes");
@@ -158,17 +158,19 @@ int real_exec(mfft_plan* plan, const void* in, void* out, int64_t batch, int fla
         if (st) return st;
         tw = t2;
     }
-    const size_t real_b = (size_t)batch * plan->n * sizeof(float);
-    const size_t cplx_b = (size_t)batch * (plan->n / 2 + 1) * sizeof(float2);
-    auto body = [&](const void* di, void* dout, cudaStream_t s) -> int {
-        if (forward) k->r2c(dim3((unsigned)ctas), s, (const float*)di, (float2*)dout, batch, tw);
-        else k->c2r(dim3((unsigned)ctas), s, (const float2*)di, (float*)dout, batch, tw);
+    const size_t real_line = (size_t)plan->n * sizeof(float);
+    const size_t cplx_line = (size_t)(plan->n / 2 + 1) * sizeof(float2);
+    auto body = [&](const void* di, void* dout, int64_t nl, cudaStream_t s) -> int {
+        const long long ctas = ((nl + 1) / 2 + k->lines - 1) / k->lines;
+        if (forward) k->r2c(dim3((unsigned)ctas), s, (const float*)di, (float2*)dout, nl, tw);
+        else k->c2r(dim3((unsigned)ctas), s, (const float2*)di, (float*)dout, nl, tw);
         cudaError_t le = cudaGetLastError();
         return le == cudaSuccess ? (int)MFFT_SUCCESS : cuda_error(le, "real FFT launch");
     };
-    if (flags == MFFT_DEVICE_MEMORY) return body(in, out, (cudaStream_t)stream);
-    return run_host_staged(plan->ctx, in, out, forward ? real_b : cplx_b, forward ? cplx_b : real_b,
-                           [&](void* di, void* dout, cudaStream_t s) { return body(di, dout, s); });
+    if (flags == MFFT_DEVICE_MEMORY) return body(in, out, batch, (cudaStream_t)stream);
+    // line pairs share a transform, so chunks start on even lines
+    return run_host_lines(plan->ctx, in, out, batch, forward ? real_line : cplx_line,
+                          forward ? cplx_line : real_line, body, false, true);
 }
 
 }  // namespace

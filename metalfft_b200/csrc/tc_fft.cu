@@ -468,11 +468,11 @@ extern "C" int mfft_exec_c2c_tc(mfft_plan* plan, const void* in, void* out, int6
     }
     if (flags == MFFT_DEVICE_MEMORY)
         return tc_launch(plan, (const float2*)in, (float2*)out, batch, direction, variant, (cudaStream_t)stream);
-    size_t bytes = (size_t)batch * TC_N * sizeof(float2);
-    return run_host_staged(
-        plan->ctx, in, out, bytes, bytes,
-        [&](void* di, void* dout, cudaStream_t s) {
-            return tc_launch(plan, (const float2*)di, (float2*)dout, batch, direction, variant, s);
+    const size_t line = (size_t)TC_N * sizeof(float2);
+    return run_host_lines(
+        plan->ctx, in, out, batch, line, line,
+        [&](const void* di, void* dout, int64_t nl, cudaStream_t s) {
+            return tc_launch(plan, (const float2*)di, (float2*)dout, nl, direction, variant, s);
         },
         true);
 }

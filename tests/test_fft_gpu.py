@@ -282,3 +282,45 @@ def test_real_input_fft_device_and_errors(M):
     with pytest.raises(M.FFTError) as e:
         f.forward_real(np.zeros(n - 1, np.float32))
     assert e.value.case == "invalidInputSize"
+
+
+@pytest.mark.parametrize("kind,n,b", [("c2c", 4096, 2000), ("c2c", 1 << 20, 5), ("c2c", 64, 70001),
+                                      ("tc", 4096, 1500), ("r2c", 16384, 1001), ("c2r", 16384, 1001),
+                                      ("r2c", 4096, 4097)])
+def test_host_arrays_across_staging_chunks(M, kind, n, b):
+    # host-array calls move through 16 MiB staging chunks on separate upload /
+    # download streams; every chunk's result equals the device-pointer call
+    import ctypes
+    import torch
+    f = M.MetalFFT(n)
+    rng = np.random.default_rng(n + b)
+    P = lambda a: ctypes.c_void_p(a.data_ptr())  # noqa: E731
+    if kind in ("c2c", "tc"):
+        x = torch.from_numpy(rng.standard_normal((b, n, 2), dtype=np.float32)).view(torch.complex64)[..., 0]
+        shape_out, dt_out = (b, n), torch.complex64
+    elif kind == "r2c":
+        x = torch.from_numpy(rng.standard_normal((b, n), dtype=np.float32))
+        shape_out, dt_out = (b, n // 2 + 1), torch.complex64
+    else:
+        x = torch.from_numpy(rng.standard_normal((b, n // 2 + 1, 2), dtype=np.float32)).view(torch.complex64)[..., 0]
+        shape_out, dt_out = (b, n), torch.float32
+    x = x.contiguous()
+
+    def run(src, dst, flags):
+        if kind == "c2c":
+            return M.lib.mfft_exec_c2c(f._plan, P(src), P(dst), b, M.FORWARD, flags, None)
+        if kind == "tc":
+            return M.lib.mfft_exec_c2c_tc(f._plan, P(src), P(dst), b, M.FORWARD, 1, flags, None)
+        fn = M.lib.mfft_exec_r2c if kind == "r2c" else M.lib.mfft_exec_c2r
+        return fn(f._plan, P(src), P(dst), b, flags, None)
+
+    xd = x.cuda()
+    yd = torch.empty(shape_out, dtype=dt_out, device="cuda")
+    M._check(run(xd, yd, M.DEVICE))
+    torch.cuda.synchronize()
+    ref = yd.cpu()
+    for pinned in (False, True):
+        xs = x.pin_memory() if pinned else x
+        yh = torch.empty(shape_out, dtype=dt_out, pin_memory=pinned)
+        M._check(run(xs, yh, M.HOST))
+        assert torch.equal(yh, ref), (kind, n, b, pinned)
