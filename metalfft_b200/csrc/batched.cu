@@ -24,6 +24,31 @@ __global__ void k_twiddle_rows(float2* tw, int off, int ns, int radix, int rowle
     tw[off + idx] = make_float2((float)c, (float)s);
 }
 
+// Programmatic dependent launch: a kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization is set up while the
+// previous kernel on the stream drains; grid_dep_wait() (before the first
+// global access) returns once that kernel has completed and its memory is
+// visible, and is a no-op for an ordinary launch.  The previous kernel
+// triggers implicitly at its end: an explicit early trigger let the next
+// grid's CTAs take SM slots too soon (N=4096 x 256 forward + inverse: 11 %
+// slower; the implicit trigger: 2 % faster than no PDL).
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <class K, class... Args>
+static cudaError_t launch_pdl(K kernel, unsigned blocks, int threads, int smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <int N, int E, int FPB, bool INV>
 __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
     k_fft_batched(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
@@ -37,6 +62,7 @@ __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
     const bool ok = f < batch;
     const PadLine buf{smem + lf * spad_size(N)};
     float2 v[E];
+    grid_dep_wait();
     if (ok) {
         const float2* src = in + (size_t)f * N + t;
 #pragma unroll
@@ -71,8 +97,7 @@ static cudaError_t launch_batched(const float2* in, float2* out, long long batch
     long long blocks = (batch + FPB - 1) / FPB;
     if (blocks <= 0) return cudaSuccess;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-    k_fft_batched<N, E, FPB, INV><<<(unsigned)blocks, threads, smem, s>>>(in, out, batch, tw);
-    return cudaGetLastError();
+    return launch_pdl(k_fft_batched<N, E, FPB, INV>, (unsigned)blocks, threads, smem, s, in, out, batch, tw);
 }
 
 template <class K>
@@ -125,6 +150,9 @@ __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
 #pragma unroll
         for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
         fence_proxy_async_smem();
+    }
+    grid_dep_wait();  // every thread: the previous kernel's writes are visible
+    if (threadIdx.x == 0) {
 #pragma unroll
         for (int s = 0; s < STAGES; ++s) {
             const long long g = blockIdx.x + (long long)s * gridDim.x;
@@ -198,8 +226,8 @@ static cudaError_t launch_stream(const float2* in, float2* out, long long batch,
     if (groups <= 0) return cudaSuccess;
     long long blocks = (long long)device_sms() * occ;
     if (blocks > groups) blocks = groups;
-    k_fft_stream<N, E, FPB, STAGES, INV><<<(unsigned)blocks, threads, smem, s>>>(in, out, batch, tw, dev_err);
-    return cudaGetLastError();
+    return launch_pdl(k_fft_stream<N, E, FPB, STAGES, INV>, (unsigned)blocks, threads, smem, s, in, out, batch, tw,
+                      dev_err);
 }
 
 template <int N, int E, int FPB, int STAGES>
