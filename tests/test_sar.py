@@ -185,8 +185,10 @@ def test_focus_matches_fp64_chain(M, reference_signs):
 @pytest.mark.gpu
 def test_focused_point_targets_meet_reference_checks(M):
     """Point targets focus at their expected bins with SNR > 10 dB
-    (src/radar/main.swift:213-218), measured with the restated
-    RadarMetrics (radar_metrics.swift:57-268)."""
+    (src/radar/main.swift:213-218) and range PSLR < -13 dB
+    (src/radar/precision_comparison.swift:587-597), measured with the restated
+    RadarMetrics (radar_metrics.swift:57-268); an unweighted chirp's first
+    sidelobe is -13.26 dB."""
     import torch
     from metalfft_b200._sar import expected_bins, point_target_metrics
     prm = M.SARParameters.default(1024, 4096, 512, 256.0)
@@ -204,7 +206,7 @@ def test_focused_point_targets_meet_reference_checks(M):
         assert abs(m["range_bin"] - rg) <= 1, (m, rg)
         assert abs(m["azimuth_bin"] - az) <= 12, (m, az)
         assert m["snr"] > 10.0, m
-        assert m["pslr_range"] < -10.0, m
+        assert m["pslr_range"] < -13.0, m
 
 
 def test_oracle_focus_signs():
