@@ -20,6 +20,8 @@
 // Output is in natural order, as the reference's last transpose leaves it
 // (src/fft_multisize_host.swift:155-164).  Inverse: conjugate on the column
 // load, conjugate and scale on the row store (MetalFFT.swift:56-65).
+#include <cudaTypedefs.h>
+
 #include "capi_internal.h"
 #include "fsqueue.h"
 #include "stockham.cuh"
@@ -91,7 +93,41 @@ void fourstep_plan_release(mfft_plan* p) {
     p->fs.tables = nullptr;
 }
 
-// Column pass then row pass over chunks of up to scratch_lines transforms.
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link-time dependency on the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        tried = true;
+    }
+    return fn;
+}
+
+// `rows` rows of `row_points` complex values at `base`, as floats; boxes of
+// `tile_cols` complex columns x 256 rows, swizzled like the item tiles
+static bool encode_rows(CUtensorMap* map, const float2* base, uint64_t rows, uint64_t row_points, int tile_cols) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {2 * row_points, rows};
+    const cuuint64_t strides[1] = {row_points * sizeof(float2)};
+    const cuuint32_t box[2] = {(cuuint32_t)(2 * tile_cols), 256};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUtensorMapSwizzle sw = tile_cols == 4   ? CU_TENSOR_MAP_SWIZZLE_32B
+                                  : tile_cols == 8 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                                   : CU_TENSOR_MAP_SWIZZLE_128B;
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float2*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Column pass then row pass over chunks of up to scratch_lines transforms;
+// n = 2^16 .. 2^20 move their tiles with TMA (tile widths 4, 8 or 16).
 int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, int direction, cudaStream_t s) {
     const FourStep& fs = p->fs;
     const int logn = ilog2c(p->n);
@@ -108,15 +144,25 @@ int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, in
         const long long nb = batch - b0 < fs.scratch_lines ? batch - b0 : fs.scratch_lines;
         a.in = in + b0 * p->n;
         a.out = out + b0 * p->n;
+        const bool tma = logn >= 16 && logn <= 20;
+        FsqMaps mc{}, mr{};
+        if (tma) {
+            const int C = FSQ_POINTS / fs.n1, RW = FSQ_POINTS / fs.n2;
+            if (!encode_rows(&mc.ld, a.in, (uint64_t)nb * fs.n1, fs.n2, C) ||
+                !encode_rows(&mc.st, a.scratch, (uint64_t)nb * fs.n1, fs.n2, C) ||
+                !encode_rows(&mr.st, a.out, (uint64_t)nb * fs.n2, fs.n1, RW))
+                return set_error(MFFT_ERR_LIBRARY_BUILD, -1, -1, -1, "four-step tensor maps could not be encoded");
+        }
         a.u_kind = FSQ_COLS;
         a.u_per = nc;
         a.nitems = (int)(nb * nc);
-        cudaError_t e = fsq_launch(a, inv, p->ctx->sms, s);
+        cudaError_t e = tma ? fsq_launch_tma(a, mc, inv, p->ctx->sms, p->ctx->dev_err, s)
+                            : fsq_launch(a, inv, p->ctx->sms, s);
         if (e == cudaSuccess) {
             a.u_kind = FSQ_ROWS;
             a.u_per = nr;
             a.nitems = (int)(nb * nr);
-            e = fsq_launch(a, inv, p->ctx->sms, s);
+            e = tma ? fsq_launch_tma(a, mr, inv, p->ctx->sms, p->ctx->dev_err, s) : fsq_launch(a, inv, p->ctx->sms, s);
         }
         if (e != cudaSuccess) return cuda_error(e, "four-step launch");
     }

@@ -127,7 +127,7 @@ __device__ __forceinline__ float2 tw_n(const float2* __restrict__ fine, const fl
     return cmul(__ldg(fine + (e & 1023u)), __ldg(coarse + (e >> 10)));
 }
 
-template <int L, bool INV>
+template <int L, bool INV, bool TILE_OUT = false>
 __device__ __forceinline__ void do_cols(float2* st, float2* __restrict__ mid, int ln2, int col0,
                                         const float2* __restrict__ tw, const float2* __restrict__ fine,
                                         const float2* __restrict__ coarse) {
@@ -167,10 +167,10 @@ __device__ __forceinline__ void do_cols(float2* st, float2* __restrict__ mid, in
 #pragma unroll
     for (int m = 0; m < 16; ++m) st[tidx(t + m * T, c, LC)] = v[m];
     __syncthreads();
-    store_tile<false>(st, mid + col0, LL, LC, 1LL << ln2);
+    if constexpr (!TILE_OUT) store_tile<false>(st, mid + col0, LL, LC, 1LL << ln2);
 }
 
-template <int L, bool INV>
+template <int L, bool INV, bool TILE_OUT = false>
 __device__ __forceinline__ void do_rows(float2* st, const float2* mid_rows, float2* __restrict__ out, int ln1,
                                         int row0, const float2* __restrict__ tw, float scale) {
     constexpr int T = L / 16, RW = FSQ_POINTS / L, LR = ilog2c(RW), LL = ilog2c(L);
@@ -188,7 +188,7 @@ __device__ __forceinline__ void do_rows(float2* st, const float2* mid_rows, floa
     for (int m = 0; m < 16; ++m)
         st[tidx(t + m * T, r, LR)] = INV ? make_float2(v[m].x * scale, -v[m].y * scale) : v[m];
     __syncthreads();
-    store_tile<true>(st, out + row0, LL, LR, 1LL << ln1);
+    if constexpr (!TILE_OUT) store_tile<true>(st, out + row0, LL, LR, 1LL << ln1);
 }
 
 // ---- items ----------------------------------------------------------------------
@@ -241,7 +241,7 @@ __device__ __forceinline__ void issue(const FsqArgs& a, const Work& w, float2* s
     }
 }
 
-template <bool INV>
+template <bool INV, bool TILE_OUT = false>
 __device__ __forceinline__ void compute(const FsqArgs& a, const Work& w, float2* st) {
     if (w.kind == FSQ_LINES) {
         const float2* tw = a.tabs.line_tw[w.logn - 6];
@@ -264,11 +264,11 @@ __device__ __forceinline__ void compute(const FsqArgs& a, const Work& w, float2*
         const float2* coarse = a.tabs.coarse[w.logn - 13];
         const int col0 = w.index << (ilog2c(FSQ_POINTS) - l1);
         switch (l1) {
-            case 6: do_cols<64, INV>(st, mid, l2, col0, tw, fine, coarse); break;
-            case 7: do_cols<128, INV>(st, mid, l2, col0, tw, fine, coarse); break;
-            case 8: do_cols<256, INV>(st, mid, l2, col0, tw, fine, coarse); break;
-            case 9: do_cols<512, INV>(st, mid, l2, col0, tw, fine, coarse); break;
-            default: do_cols<1024, INV>(st, mid, l2, col0, tw, fine, coarse); break;
+            case 6: do_cols<64, INV, TILE_OUT>(st, mid, l2, col0, tw, fine, coarse); break;
+            case 7: do_cols<128, INV, TILE_OUT>(st, mid, l2, col0, tw, fine, coarse); break;
+            case 8: do_cols<256, INV, TILE_OUT>(st, mid, l2, col0, tw, fine, coarse); break;
+            case 9: do_cols<512, INV, TILE_OUT>(st, mid, l2, col0, tw, fine, coarse); break;
+            default: do_cols<1024, INV, TILE_OUT>(st, mid, l2, col0, tw, fine, coarse); break;
         }
     } else {
         const float2* tw = a.tabs.line_tw[l2 - 6];
@@ -277,10 +277,10 @@ __device__ __forceinline__ void compute(const FsqArgs& a, const Work& w, float2*
         float2* dst = a.out + w.off;
         const float scale = 1.0f / (float)(1LL << w.logn);
         switch (l2) {
-            case 7: do_rows<128, INV>(st, rows, dst, l1, row0, tw, scale); break;
-            case 8: do_rows<256, INV>(st, rows, dst, l1, row0, tw, scale); break;
-            case 9: do_rows<512, INV>(st, rows, dst, l1, row0, tw, scale); break;
-            default: do_rows<1024, INV>(st, rows, dst, l1, row0, tw, scale); break;
+            case 7: do_rows<128, INV, TILE_OUT>(st, rows, dst, l1, row0, tw, scale); break;
+            case 8: do_rows<256, INV, TILE_OUT>(st, rows, dst, l1, row0, tw, scale); break;
+            case 9: do_rows<512, INV, TILE_OUT>(st, rows, dst, l1, row0, tw, scale); break;
+            default: do_rows<1024, INV, TILE_OUT>(st, rows, dst, l1, row0, tw, scale); break;
         }
     }
 }
@@ -309,11 +309,135 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM) k_fsq(const FsqA
     cp_async_wait<0>();
 }
 
+
+// ---- TMA form of the uniform four-step passes (n = 2^16 .. 2^20) -------------
+//
+// For these sizes every tile is 4, 8 or 16 columns wide (32-, 64- or 128-byte
+// rows), and the chunk-pair swizzle of tidx() is exactly the TMA swizzle of
+// that row width (SWIZZLE_32B / 64B / 128B: 16-byte chunk index XOR address
+// bits 7..9).  So the tiles move with tensor copies issued by one thread:
+// column items load n1/256 boxes of C columns x 256 rows from the input and
+// store their finished tile to the intermediate the same way; row items load
+// their 4096 contiguous points with one 1-D bulk copy and store the transposed
+// tile as boxes of RW columns x 256 rows of the output.  Loads complete on a
+// per-stage mbarrier (bounded wait); a stage is refilled only after the bulk
+// store that read it has finished reading.
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int y, const void* src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+constexpr int TMA_BOX_ROWS = 256;
+
+// thread 0: item p's data into stage `st`, counted on `bar`
+__device__ __forceinline__ void tma_issue(const FsqArgs& a, const FsqMaps& m, const Work& w, float2* st,
+                                          uint64_t* bar) {
+    const int l1 = w.logn / 2, l2 = w.logn - l1;
+    mbar_arrive_expect_tx(bar, FSQ_POINTS * (uint32_t)sizeof(float2));
+    const long long j = w.off >> w.logn;  // transform index in this chunk
+    if (w.kind == FSQ_COLS) {
+        const int lc = ilog2c(FSQ_POINTS) - l1;
+        const int x = (w.index << lc) * 2;  // floats
+        const int C = 1 << lc;
+        for (int k = 0; k < (1 << l1) / TMA_BOX_ROWS; ++k)
+            tma_load_2d(st + k * TMA_BOX_ROWS * C, &m.ld, x, (int)(j << l1) + k * TMA_BOX_ROWS, bar);
+    } else {
+        const int lr = ilog2c(FSQ_POINTS) - l2;
+        bulk_g2s(st, a.scratch + w.scratch + ((long long)w.index << (lr + l2)), FSQ_POINTS * (uint32_t)sizeof(float2),
+                 bar);
+    }
+}
+
+// thread 0: the finished tile of item w from stage `st`
+__device__ __forceinline__ void tma_store(const FsqMaps& m, const Work& w, const float2* st) {
+    const int l1 = w.logn / 2, l2 = w.logn - l1;
+    const long long j = w.off >> w.logn;
+    if (w.kind == FSQ_COLS) {
+        const int lc = ilog2c(FSQ_POINTS) - l1, C = 1 << lc;
+        const int x = (w.index << lc) * 2;
+        for (int k = 0; k < (1 << l1) / TMA_BOX_ROWS; ++k)
+            tma_store_2d(&m.st, x, (int)(j << l1) + k * TMA_BOX_ROWS, st + k * TMA_BOX_ROWS * C);
+    } else {
+        const int lr = ilog2c(FSQ_POINTS) - l2, RW = 1 << lr;
+        const int x = (w.index << lr) * 2;  // first row of the group = first output column
+        for (int k = 0; k < (1 << l2) / TMA_BOX_ROWS; ++k)
+            tma_store_2d(&m.st, x, (int)(j << l2) + k * TMA_BOX_ROWS, st + k * TMA_BOX_ROWS * RW);
+    }
+    bulk_commit();
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
+    k_fsq_tma(const __grid_constant__ FsqArgs a, const __grid_constant__ FsqMaps m, int* dev_err) {
+    extern __shared__ __align__(1024) unsigned char fsq_raw[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int abort_sh;
+    // swizzled tiles need 1024-byte aligned stages (the stage size is 34 KiB)
+    float2* smem = reinterpret_cast<float2*>(fsq_raw + ((1024u - (smem_u32(fsq_raw) & 1023u)) & 1023u));
+    int p = blockIdx.x;
+    if (p >= a.nitems) return;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        abort_sh = 0;
+        fence_proxy_async_smem();
+        tma_issue(a, m, get_work(a, p), smem, &bar[0]);
+    }
+    __syncthreads();
+    int s = 0;
+    uint32_t ph[2] = {0u, 0u};
+    for (; p < a.nitems; p += gridDim.x) {
+        const int q = p + gridDim.x;
+        if (threadIdx.x == 0 && q < a.nitems) {
+            bulk_wait_read_all();  // the store that last read stage s^1 has read it
+            tma_issue(a, m, get_work(a, q), smem + (s ^ 1) * QSTAGE, &bar[s ^ 1]);
+        }
+        if (!mbar_wait(&bar[s], ph[s])) abort_sh = 1;
+        ph[s] ^= 1u;
+        __syncthreads();
+        if (abort_sh) break;
+        const Work w = get_work(a, p);
+        compute<INV, true>(a, w, smem + s * QSTAGE);
+        fence_proxy_async_smem();  // the tile's generic writes before the bulk store reads them
+        __syncthreads();
+        if (threadIdx.x == 0) tma_store(m, w, smem + s * QSTAGE);
+        s ^= 1;
+    }
+    if (threadIdx.x == 0) {
+        if (abort_sh) {
+            report_device_error(dev_err, DEV_ERR_TMA_TIMEOUT);
+            // copies still in flight land before the CTA's shared memory goes away
+            mbar_wait(&bar[0], ph[0]);
+            mbar_wait(&bar[1], ph[1]);
+        }
+        bulk_wait_all();
+    }
+}
+
 }  // namespace
 
 cudaError_t fsq_prepare() {
     for (auto k : {k_fsq<false>, k_fsq<true>}) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, QSMEM);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+    }
+    for (auto k : {k_fsq_tma<false>, k_fsq_tma<true>}) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, QSMEM + 1024);
         if (e != cudaSuccess) return e;
         e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess) return e;
@@ -327,6 +451,15 @@ cudaError_t fsq_launch(const FsqArgs& a, bool inverse, int sms, cudaStream_t s) 
     if (grid > a.nitems) grid = a.nitems;
     if (inverse) k_fsq<true><<<(unsigned)grid, FSQ_THREADS, QSMEM, s>>>(a);
     else k_fsq<false><<<(unsigned)grid, FSQ_THREADS, QSMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t fsq_launch_tma(const FsqArgs& a, const FsqMaps& m, bool inverse, int sms, int* dev_err, cudaStream_t s) {
+    if (a.nitems <= 0) return cudaSuccess;
+    long long grid = (long long)sms * FSQ_CTAS_PER_SM;
+    if (grid > a.nitems) grid = a.nitems;
+    if (inverse) k_fsq_tma<true><<<(unsigned)grid, FSQ_THREADS, QSMEM + 1024, s>>>(a, m, dev_err);
+    else k_fsq_tma<false><<<(unsigned)grid, FSQ_THREADS, QSMEM + 1024, s>>>(a, m, dev_err);
     return cudaGetLastError();
 }
 

@@ -18,6 +18,7 @@
 // another inside a launch and no inter-CTA synchronisation exists.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace mfft {
@@ -82,8 +83,20 @@ inline int fsq_rows_items(int logn) {
     return n1 / (FSQ_POINTS / n2);
 }
 
+// Tensor maps of a uniform pass with TMA tiles: ld = the input viewed as
+// rows of n2 points (column pass), st = the column pass's intermediate (rows
+// of n2) or the row pass's output (rows of n1, transposed store).  Float
+// elements, boxes of (2 x tile width) floats x 256 rows, swizzle of the tile
+// row width.
+struct FsqMaps {
+    CUtensorMap ld;
+    CUtensorMap st;
+};
+
 cudaError_t fsq_prepare();
 // Launches one pass over a.nitems items on `s`.
 cudaError_t fsq_launch(const FsqArgs& a, bool inverse, int sms, cudaStream_t s);
+// The same uniform pass with TMA tiles (four-step n = 2^16 .. 2^20 only).
+cudaError_t fsq_launch_tma(const FsqArgs& a, const FsqMaps& m, bool inverse, int sms, int* dev_err, cudaStream_t s);
 
 }  // namespace mfft
