@@ -118,6 +118,14 @@ int line_twiddles(mfft_ctx* ctx, int n, float2** out);
 // built on the context's stream; the caller owns the allocation.
 int fourstep_tables(mfft_ctx* ctx, int64_t n, float2** out);
 
+// Four-step sizes whose tiles move by TMA (2^16 .. 2^20), and one pass
+// (FSQ_COLS or FSQ_ROWS) of them over nb contiguous transforms of 2^logn
+// points: in / out / scratch are the first transform's data (fsqueue.h).
+bool fsq_tma_size(int logn);
+struct FsqTables;
+int fourstep_tma_pass(int kind, const FsqTables& tabs, const float2* in, float2* out, float2* scratch, long long nb,
+                      int logn, bool inv, mfft_ctx* ctx, cudaStream_t s);
+
 int fourstep_plan_init(mfft_plan* plan);
 void fourstep_plan_release(mfft_plan* plan);
 int fourstep_exec(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,

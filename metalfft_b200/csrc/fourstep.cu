@@ -126,6 +126,35 @@ static bool encode_rows(CUtensorMap* map, const float2* base, uint64_t rows, uin
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+bool fsq_tma_size(int logn) { return logn >= 16 && logn <= 20; }
+
+int fourstep_tma_pass(int kind, const FsqTables& tabs, const float2* in, float2* out, float2* scratch, long long nb,
+                      int logn, bool inv, mfft_ctx* ctx, cudaStream_t s) {
+    int n1, n2;
+    fsq_split(logn, &n1, &n2);
+    FsqArgs a{};
+    a.in = in;
+    a.out = out;
+    a.scratch = scratch;
+    a.u_logn = logn;
+    a.tabs = tabs;
+    FsqMaps m{};
+    bool ok;
+    if (kind == FSQ_COLS) {
+        const int C = FSQ_POINTS / n1;
+        ok = encode_rows(&m.ld, in, (uint64_t)nb * n1, n2, C) && encode_rows(&m.st, scratch, (uint64_t)nb * n1, n2, C);
+        a.u_per = fsq_cols_items(logn);
+    } else {
+        ok = encode_rows(&m.st, out, (uint64_t)nb * n2, n1, FSQ_POINTS / n2);
+        a.u_per = fsq_rows_items(logn);
+    }
+    if (!ok) return set_error(MFFT_ERR_LIBRARY_BUILD, -1, -1, -1, "four-step tensor maps could not be encoded");
+    a.u_kind = kind;
+    a.nitems = (int)(nb * a.u_per);
+    cudaError_t e = fsq_launch_tma(a, m, inv, ctx->sms, ctx->dev_err, s);
+    return e == cudaSuccess ? (int)MFFT_SUCCESS : cuda_error(e, "four-step launch");
+}
+
 // Column pass then row pass over chunks of up to scratch_lines transforms;
 // n = 2^16 .. 2^20 move their tiles with TMA (tile widths 4, 8 or 16).
 int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, int direction, cudaStream_t s) {
@@ -144,25 +173,21 @@ int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, in
         const long long nb = batch - b0 < fs.scratch_lines ? batch - b0 : fs.scratch_lines;
         a.in = in + b0 * p->n;
         a.out = out + b0 * p->n;
-        const bool tma = logn >= 16 && logn <= 20;
-        FsqMaps mc{}, mr{};
-        if (tma) {
-            const int C = FSQ_POINTS / fs.n1, RW = FSQ_POINTS / fs.n2;
-            if (!encode_rows(&mc.ld, a.in, (uint64_t)nb * fs.n1, fs.n2, C) ||
-                !encode_rows(&mc.st, a.scratch, (uint64_t)nb * fs.n1, fs.n2, C) ||
-                !encode_rows(&mr.st, a.out, (uint64_t)nb * fs.n2, fs.n1, RW))
-                return set_error(MFFT_ERR_LIBRARY_BUILD, -1, -1, -1, "four-step tensor maps could not be encoded");
+        if (fsq_tma_size(logn)) {
+            int st = fourstep_tma_pass(FSQ_COLS, a.tabs, a.in, a.out, a.scratch, nb, logn, inv, p->ctx, s);
+            if (!st) st = fourstep_tma_pass(FSQ_ROWS, a.tabs, a.in, a.out, a.scratch, nb, logn, inv, p->ctx, s);
+            if (st) return st;
+            continue;
         }
         a.u_kind = FSQ_COLS;
         a.u_per = nc;
         a.nitems = (int)(nb * nc);
-        cudaError_t e = tma ? fsq_launch_tma(a, mc, inv, p->ctx->sms, p->ctx->dev_err, s)
-                            : fsq_launch(a, inv, p->ctx->sms, s);
+        cudaError_t e = fsq_launch(a, inv, p->ctx->sms, s);
         if (e == cudaSuccess) {
             a.u_kind = FSQ_ROWS;
             a.u_per = nr;
             a.nitems = (int)(nb * nr);
-            e = tma ? fsq_launch_tma(a, mr, inv, p->ctx->sms, p->ctx->dev_err, s) : fsq_launch(a, inv, p->ctx->sms, s);
+            e = fsq_launch(a, inv, p->ctx->sms, s);
         }
         if (e != cudaSuccess) return cuda_error(e, "four-step launch");
     }

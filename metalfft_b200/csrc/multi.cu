@@ -10,6 +10,10 @@
 //            the tail of the launch;
 //   pass 1   the ROWS items of every four-step transform (absent when there
 //            is none).
+// Four-step classes of 2^16 .. 2^20 points skip the lists: their transforms
+// are contiguous, so each class runs the uniform passes whose tiles move by
+// TMA (fourstep.cu), its column pass after list pass 0 and its row pass after
+// list pass 1.
 #include <algorithm>
 #include <vector>
 
@@ -28,6 +32,12 @@ struct mfft_multi {
     int nitems0 = 0, nitems1 = 0;
     FsqTables tabs{};
     std::vector<float2*> tables;  // owned four-step W_n tables
+    struct Group {                // a four-step class run by the TMA passes
+        int64_t offset, count;
+        int logn;
+        long long scratch;
+    };
+    std::vector<Group> groups;
 };
 
 extern "C" int mfft_multi_destroy(mfft_multi* m) {
@@ -101,6 +111,11 @@ extern "C" int mfft_multi_create(mfft_ctx* ctx, const mfft_multi_desc* descs, in
             m->tabs.fine[logn - 13] = t;
             m->tabs.coarse[logn - 13] = t + 1024;
         }
+        if (fsq_tma_size(logn)) {
+            m->groups.push_back(mfft_multi::Group{d.offset, d.count, logn, scratch_pts});
+            scratch_pts += d.n * d.count;
+            continue;
+        }
         const int nc = fsq_cols_items(logn), nr = fsq_rows_items(logn);
         for (int64_t j = 0; j < d.count; ++j) {
             const int id = (int)xfs.size();
@@ -156,12 +171,23 @@ static int multi_device(mfft_multi* m, const float2* in, float2* out, int direct
     a.tabs = m->tabs;
     const bool inv = direction == MFFT_INVERSE;
     cudaError_t e = fsq_launch(a, inv, m->ctx->sms, s);
-    if (e == cudaSuccess && m->nitems1) {
+    if (e != cudaSuccess) return cuda_error(e, "mixed-size launch");
+    for (const auto& g : m->groups) {
+        int st = fourstep_tma_pass(FSQ_COLS, m->tabs, in + g.offset, out + g.offset, m->scratch + g.scratch, g.count,
+                                   g.logn, inv, m->ctx, s);
+        if (st) return st;
+    }
+    if (m->nitems1) {
         a.items = m->d_items + m->nitems0;
         a.nitems = m->nitems1;
         e = fsq_launch(a, inv, m->ctx->sms, s);
+        if (e != cudaSuccess) return cuda_error(e, "mixed-size launch");
     }
-    if (e != cudaSuccess) return cuda_error(e, "mixed-size launch");
+    for (const auto& g : m->groups) {
+        int st = fourstep_tma_pass(FSQ_ROWS, m->tabs, in + g.offset, out + g.offset, m->scratch + g.scratch, g.count,
+                                   g.logn, inv, m->ctx, s);
+        if (st) return st;
+    }
     return MFFT_SUCCESS;
 }
 

@@ -233,3 +233,18 @@ def test_mixed_host_arrays(M):
         for j in range(c):
             seg = slice(off + j * n, off + (j + 1) * n)
             assert O.rel_rms(y[seg][None], O.truth(x[seg][None])) < 3e-6
+
+
+def test_mixed_in_place_matches_out_of_place(M):
+    # in == out: the row passes, which write the four-step outputs, run after
+    # every column pass has read its input (item lists and TMA classes alike)
+    import torch
+    classes = [(256, 7), (4096, 3), (8192, 2), (1 << 15, 1), (1 << 16, 2), (1 << 18, 1), (1 << 20, 2)]
+    mb = M.MixedBatch(classes)
+    x = torch.from_numpy(O.normal_c64((mb.points,), 41)).cuda()
+    y = torch.empty_like(x)
+    mb.exec(x, y, M.FORWARD)
+    z = x.clone()
+    mb.exec(z, z, M.FORWARD)
+    torch.cuda.synchronize()
+    assert torch.equal(y, z)
