@@ -228,9 +228,10 @@ class _Desc(ctypes.Structure):
 
 
 class MixedBatch:
-    """Transforms of several sizes in one persistent launch (no reference
-    counterpart).  sizes_counts: [(n, count), ...]; transforms of a class are
-    stored back to back, classes one after another in the given order."""
+    """Transforms of several sizes in a few launches of the persistent item
+    kernel (no reference counterpart).  sizes_counts: [(n, count), ...];
+    transforms of a class are stored back to back, classes one after another
+    in the given order."""
 
     def __init__(self, sizes_counts, context=None):
         descs = (_Desc * len(sizes_counts))()
@@ -255,6 +256,16 @@ class MixedBatch:
         """Device tensors (torch complex64, `points` elements)."""
         _check(lib.mfft_multi_exec(self._h, _ptr(inp), _ptr(out), direction, DEVICE, _stream_of(inp)))
         return out
+
+    def capture(self, inp, out, direction=FORWARD):
+        """One CUDA graph of exec(inp, out, direction): every launch of the
+        batch replays with one graph launch.  The tensors must stay alive and
+        in place."""
+        import torch
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.exec(inp, out, direction)
+        return g
 
     def forward(self, x):
         if _is_cuda_tensor(x):
