@@ -35,6 +35,7 @@ using FhPlan = SPlan<FH_N, FH_E>;
 __device__ __forceinline__ __half2 h2(float2 a) { return __float22half2_rn(a); }
 __device__ __forceinline__ float2 f2(__half2 a) { return __half22float2(a); }
 __device__ __forceinline__ float2 round_h(float2 a) { return f2(h2(a)); }
+__device__ __forceinline__ int hpad(int i) { return i + (i >> 5); }
 // complex product in FP16
 __device__ __forceinline__ __half2 hcmul(__half2 a, __half2 b) { return __hcmadd(a, b, __float2half2_rn(0.f)); }
 
@@ -149,7 +150,8 @@ __device__ __forceinline__ void htwiddle(typename A::V (&v)[FH_E], const float2*
 
 // pass P of the 3-pass radix-16 Stockham FFT of 4096 points, 256 threads:
 // on entry v[m] = element t + 256 m of the pass input; exchanges through the
-// half2 line `buf` (padded index spad)
+// half2 line `buf` (padded index hpad: one spare 4-byte slot per 32, so a
+// warp reading 32 consecutive elements hits 32 distinct banks)
 template <class A, int P>
 __device__ __forceinline__ void hpass(typename A::V (&v)[FH_E], int t, __half2* buf, const float2* __restrict__ tw) {
     constexpr int NS = FhPlan::span(P);
@@ -159,10 +161,10 @@ __device__ __forceinline__ void hpass(typename A::V (&v)[FH_E], int t, __half2* 
         const int k = t & (NS - 1);
         const int d = (t - k) * FH_E + k;
 #pragma unroll
-        for (int r = 0; r < FH_E; ++r) A::store(buf + spad(d + r * NS), v[r]);
+        for (int r = 0; r < FH_E; ++r) A::store(buf + hpad(d + r * NS), v[r]);
         __syncthreads();
 #pragma unroll
-        for (int m = 0; m < FH_E; ++m) v[m] = A::load(buf + spad(t + m * FH_T));
+        for (int m = 0; m < FH_E; ++m) v[m] = A::load(buf + hpad(t + m * FH_T));
         __syncthreads();
         hpass<A, P + 1>(v, t, buf, tw);
     }
@@ -183,7 +185,8 @@ struct FhPolicy<MFFT_CONV_FP16_PURE> {
     using A = ArPure;
 };
 
-constexpr int FH_SMEM = spad_size(FH_N) * 4 + 2 * FH_N * 4;  // half2 exchange + two FP32 overlap rows
+constexpr int FH_XCH = FH_N + FH_N / 32;                      // half2 slots of the exchange line
+constexpr int FH_SMEM = FH_XCH * 4 + 2 * FH_N * 4;               // half2 exchange + two FP32 overlap rows
 
 // Same walker contract as the FP32 forward kernel: unit = CTA owns block
 // pairs [p0, p1) of the nout output blocks, recomputes `warm_blocks` earlier
@@ -197,7 +200,7 @@ __global__ void __launch_bounds__(FH_T, 2)
     using V = typename A::V;
     extern __shared__ __align__(16) unsigned char fh_smem[];
     __half2* buf = reinterpret_cast<__half2*>(fh_smem);
-    float* acc0 = reinterpret_cast<float*>(fh_smem + spad_size(FH_N) * 4);
+    float* acc0 = reinterpret_cast<float*>(fh_smem + FH_XCH * 4);
     float* acc1 = acc0 + FH_N;
     const int t = threadIdx.x;
     const long long unit = blockIdx.x;
