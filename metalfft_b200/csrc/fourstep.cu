@@ -22,6 +22,8 @@
 // load, conjugate and scale on the row store (MetalFFT.swift:56-65).
 #include <cudaTypedefs.h>
 
+#include <mutex>
+
 #include "capi_internal.h"
 #include "fsqueue.h"
 #include "stockham.cuh"
@@ -97,15 +99,14 @@ void fourstep_plan_release(mfft_plan* p) {
 // link-time dependency on the driver library)
 static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
+    static std::once_flag once;
+    std::call_once(once, [] {
         void* f = nullptr;
         cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
             fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-        tried = true;
-    }
+    });
     return fn;
 }
 

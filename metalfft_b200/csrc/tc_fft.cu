@@ -385,13 +385,10 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 template <bool SPLIT, bool INV>
 cudaError_t launch_tc(const float2* in, float2* out, long long batch, const uint4* gimg, const float2* tw,
                       int* dev_err, int sms, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_fft4096_tc<SPLIT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             SM_BYTES);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    // the shared-memory opt-in is a per-device attribute: set it on the
+    // current device at every call (a few microseconds)
+    cudaError_t e = cudaFuncSetAttribute(k_fft4096_tc<SPLIT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM_BYTES);
+    if (e != cudaSuccess) return e;
     long long blocks = (long long)sms * 2;
     if (blocks > batch) blocks = batch;
     if (blocks <= 0) return cudaSuccess;
