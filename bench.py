@@ -723,7 +723,7 @@ def main():
            "h2d_bytes_per_step": B * N * 8, "d2h_bytes_per_step": B * N * 8,
            "steps": args.e2e_steps}
 
-    kernel_name = "k_fft_batched" if best == "fp32" else "k_fft4096_tc"
+    kernel_name = "k_fft_batched" if best == "fp32" else "k_fft4096_tcq"
     line = {
         "metric": METRIC,
         "value": r["transforms_per_s"],

@@ -26,13 +26,14 @@
 //               scales are undone exactly in the epilogues.
 //   BF16:       one product of bf16 operands.
 //
-// One CTA of 256 threads (8 warps) transforms one line at a time, 2 CTAs per
-// SM; the next line's loads are issued before the current line's tensor-core
-// work so they overlap it, and its maximum is published at the barrier that
-// ends the current line.  The stage-2 scale is s1/64 (a DFT-64 grows
-// magnitudes by at most 64), so no reduction sits between the two products.  The single thread that issues the MMAs waits on
-// the commit mbarrier with a time limit; a timeout sets the device error word
-// and the CTA leaves its loop, frees its TMEM and returns.
+// One CTA of 512 threads per SM holds G once and runs four independent
+// pipelines of 128 threads, one line each at a time (four lines in flight per
+// SM), each with its own B buffers, TMEM columns, commit mbarrier and named
+// barrier.  The stage-2 scale is s1/64 (a DFT-64 grows magnitudes by at most
+// 64), so no reduction sits between the two products.  A pipeline's first
+// thread issues its MMAs and waits on the commit mbarrier with a time limit;
+// a timeout sets the device error word and the pipeline leaves its loop; the
+// CTA then frees its TMEM and returns.
 #include "capi_internal.h"
 #include "fft_common.cuh"
 #include "tcgen05.cuh"
@@ -46,19 +47,12 @@ namespace {
 
 constexpr int TC_N = 4096;
 constexpr int TC_R = 64;
-constexpr int TC_THREADS = 256;
 constexpr float TC_GSCALE = 16.0f;  // FP16 split: G stored as 16 * DFT-64
 constexpr int TC_LINE_EXP = 14;     // FP16 split: line scaled so |max| < 2^14
 
 // shared-memory byte offsets from a 1024-byte aligned base (dynamic)
 constexpr uint32_t SM_G0 = 0;          // G hi (or bf16) : 128 x 128 halves = 32 KB
 constexpr uint32_t SM_G1 = 32768;      // G lo
-constexpr uint32_t SM_B0 = 65536;      // B hi (or bf16) : 128 x 64 halves = 16 KB
-constexpr uint32_t SM_B1 = 81920;      // B lo
-constexpr uint32_t SM_T1 = 98304;      // W4096^(i*k1), i < 16, k1 < 64: 8 KB
-constexpr uint32_t SM_T0 = 106496;     // W4096^(16*j*k1), j < 4, k1 < 64: 2 KB
-constexpr uint32_t SM_BYTES = 108544 + 1024;  // + alignment slack
-constexpr uint32_t TMEM_COLS = 128;    // D1: columns [0, 64), D2: [64, 128)
 
 // Operand layouts: 128-byte swizzle (1024-byte atoms of 8 rows x 128 bytes,
 // 16-byte chunk c of row r stored at chunk c ^ (r % 8)), so that the eight
@@ -116,9 +110,23 @@ __device__ __forceinline__ float line_scale(float mx) {
     return ldexpf(1.f, TC_LINE_EXP - e);
 }
 
-// 8 values -> one 16-byte chunk of hi (and lo) halves / bf16
+// ---- four pipelines per CTA -------------------------------------------------
+//
+// One CTA of 512 threads per SM holds the DFT-64 operand once and runs four
+// independent 128-thread pipelines, each with its own line, B operand buffers
+// (32 KB), TMEM columns (D1, D2), commit mbarrier and named barrier: four
+// lines in flight per SM where two CTAs of one pipeline each hold two (and
+// two copies of the operand).  A pipeline's four warps cover the 128 TMEM
+// lanes, each walking both 32-column halves of D1 and D2; lines are loaded
+// directly (no register prefetch: the other pipelines cover the latency).
+constexpr int TQ_PIPES = 4, TQ_PT = 128, TQ_THREADS = TQ_PIPES * TQ_PT;
+constexpr uint32_t TQ_B = 65536, TQ_BSTRIDE = 32768;          // pipeline p: B hi at TQ_B + p*TQ_BSTRIDE, lo +16 KB
+constexpr uint32_t TQ_T1 = TQ_B + TQ_PIPES * TQ_BSTRIDE;      // W4096^(i*k1), i < 16: 8 KB
+constexpr uint32_t TQ_T0 = TQ_T1 + 8192;                      // W4096^(16*j*k1), j < 4: 2 KB
+constexpr uint32_t TQ_SMEM = TQ_T0 + 2048 + 1024;             // + alignment slack
+
 template <bool SPLIT>
-__device__ __forceinline__ void store_chunk(uint8_t* smem, uint32_t off, const float (&x)[8]) {
+__device__ __forceinline__ void store_chunk_b(uint8_t* bhi, uint32_t off, const float (&x)[8]) {
     if constexpr (SPLIT) {
         __align__(16) __half hi[8];
         __align__(16) __half lo[8];
@@ -127,134 +135,118 @@ __device__ __forceinline__ void store_chunk(uint8_t* smem, uint32_t off, const f
             hi[i] = __float2half_rn(x[i]);
             lo[i] = __float2half_rn(x[i] - __half2float(hi[i]));
         }
-        *reinterpret_cast<uint4*>(smem + SM_B0 + off) = *reinterpret_cast<const uint4*>(hi);
-        *reinterpret_cast<uint4*>(smem + SM_B1 + off) = *reinterpret_cast<const uint4*>(lo);
+        *reinterpret_cast<uint4*>(bhi + off) = *reinterpret_cast<const uint4*>(hi);
+        *reinterpret_cast<uint4*>(bhi + 16384 + off) = *reinterpret_cast<const uint4*>(lo);
     } else {
         __align__(16) __nv_bfloat16 bf[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) bf[i] = __float2bfloat16_rn(x[i]);
-        *reinterpret_cast<uint4*>(smem + SM_B0 + off) = *reinterpret_cast<const uint4*>(bf);
+        *reinterpret_cast<uint4*>(bhi + off) = *reinterpret_cast<const uint4*>(bf);
     }
 }
 
-// D (+)= G * B over K = 128 (8 steps of 16): three products for the split.
-// K step j: K-major operands advance (j/4) atoms plus (j%4)*32 bytes inside
-// the 128-byte row; the MN-major B1 advances two 8-row groups.
+// D (+)= G * B over K = 128 with this pipeline's B planes at b_addr (lo +16 KB)
 template <bool SPLIT, bool B_MN>
-__device__ __forceinline__ void issue_product(uint32_t d_tmem, uint32_t smem_base, uint32_t idesc) {
+__device__ __forceinline__ void issue_product_q(uint32_t d_tmem, uint32_t g_addr, uint32_t b_addr, uint32_t idesc) {
     constexpr int NPROD = SPLIT ? 3 : 1;
 #pragma unroll
-    for (int p = 0; p < NPROD; ++p) {
-        const uint32_t ga = smem_base + (p == 2 ? SM_G1 : SM_G0);
-        const uint32_t bb = smem_base + (p == 1 ? SM_B1 : SM_B0);
+    for (int pr = 0; pr < NPROD; ++pr) {
+        const uint32_t ga = g_addr + (pr == 2 ? SM_G1 : SM_G0);
+        const uint32_t bb = b_addr + (pr == 1 ? 16384u : 0u);
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const uint64_t ad = tc::smem_desc(ga + (j / 4) * G_KATOM + (j % 4) * 32, 16, ATOM_SBO, tc::LAYOUT_SW128);
             const uint64_t bd =
                 B_MN ? tc::smem_desc(bb + 2 * j * ATOM_SBO, 16384, ATOM_SBO, tc::LAYOUT_SW128)
                      : tc::smem_desc(bb + (j / 4) * B2_KATOM + (j % 4) * 32, 16, ATOM_SBO, tc::LAYOUT_SW128);
-            tc::mma_f16_ss(d_tmem, ad, bd, idesc, (p > 0 || j > 0) ? 1u : 0u);
+            tc::mma_f16_ss(d_tmem, ad, bd, idesc, (pr > 0 || j > 0) ? 1u : 0u);
         }
     }
 }
 
+__device__ __forceinline__ void pipe_sync(int p) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + p), "r"(TQ_PT) : "memory");
+}
+
 template <bool SPLIT, bool INV>
-__global__ void __launch_bounds__(TC_THREADS, 2)
-    k_fft4096_tc(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
-                 const uint4* __restrict__ gimg, const float2* __restrict__ tw, int* dev_err) {
+__global__ void __launch_bounds__(TQ_THREADS, 1)
+    k_fft4096_tcq(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
+                  const uint4* __restrict__ gimg, const float2* __restrict__ tw, int* dev_err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    __shared__ __align__(8) uint64_t mbar;
+    __shared__ __align__(8) uint64_t mbar[TQ_PIPES];
     __shared__ uint32_t tmem_base_sh;
-    __shared__ float red1[TC_THREADS / 32];
-    __shared__ int abort_sh;
+    __shared__ float red1[TQ_PIPES][4];
+    __shared__ int abort_sh[TQ_PIPES];
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    // swizzle atoms need 1024-byte alignment
+    const int p = warp >> 2;              // pipeline
+    const int q = warp & 3;               // this warp's TMEM lane quarter
+    const int ptid = tid & (TQ_PT - 1);   // thread within the pipeline
     uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const uint32_t sbase = smem_u32(smem);
     constexpr uint32_t FMT = SPLIT ? 0u : 1u;
-    constexpr uint32_t IDESC1 = tc::idesc_f16(FMT, 1u, 128, 64);  // B MN-major
-    constexpr uint32_t IDESC2 = tc::idesc_f16(FMT, 0u, 128, 64);  // B K-major
+    constexpr uint32_t IDESC1 = tc::idesc_f16(FMT, 1u, 128, 64);
+    constexpr uint32_t IDESC2 = tc::idesc_f16(FMT, 0u, 128, 64);
 
-    // G planes into shared memory (32 KB per plane)
     constexpr int GWORDS = (SPLIT ? 65536 : 32768) / 16;
-    for (int i = tid; i < GWORDS; i += TC_THREADS)
-        reinterpret_cast<uint4*>(smem)[i] = __ldg(gimg + i);
-    // stage twiddles W4096^(n2*k1), n2 = 16*j + i: T0[j][k1] * T1[i][k1], so a
-    // warp (consecutive k1) reads consecutive shared-memory words
-    float2* t1 = reinterpret_cast<float2*>(smem + SM_T1);
-    float2* t0 = reinterpret_cast<float2*>(smem + SM_T0);
-    for (int i = tid; i < 16 * 64; i += TC_THREADS) t1[i] = __ldg(tw + ((i >> 6) * (i & 63)));
-    for (int i = tid; i < 4 * 64; i += TC_THREADS) t0[i] = __ldg(tw + (16 * (i >> 6) * (i & 63)));
-    if (tid == 0) {
-        mbar_init(&mbar, 1);
-        abort_sh = 0;
+    for (int i = tid; i < GWORDS; i += TQ_THREADS) reinterpret_cast<uint4*>(smem)[i] = __ldg(gimg + i);
+    float2* t1 = reinterpret_cast<float2*>(smem + TQ_T1);
+    float2* t0 = reinterpret_cast<float2*>(smem + TQ_T0);
+    for (int i = tid; i < 16 * 64; i += TQ_THREADS) t1[i] = __ldg(tw + ((i >> 6) * (i & 63)));
+    for (int i = tid; i < 4 * 64; i += TQ_THREADS) t0[i] = __ldg(tw + (16 * (i >> 6) * (i & 63)));
+    if (tid < TQ_PIPES) {
+        mbar_init(&mbar[tid], 1);
+        abort_sh[tid] = 0;
     }
     if (warp == 0) {
-        tc::tmem_alloc(&tmem_base_sh, TMEM_COLS);
+        tc::tmem_alloc(&tmem_base_sh, 512);
         tc::tmem_relinquish();
     }
     fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tmem = tmem_base_sh;
-    const uint32_t d1 = tmem, d2 = tmem + 64;
+    const uint32_t d1 = tmem_base_sh + (uint32_t)p * 128u, d2 = d1 + 64u;
+    uint8_t* bp = smem + TQ_B + (uint32_t)p * TQ_BSTRIDE;
+    const uint32_t baddr = sbase + TQ_B + (uint32_t)p * TQ_BSTRIDE;
 
-    // epilogue geometry: warp -> lane quarter q, column half h
-    const int q = warp & 3, h = warp >> 2;
-    const int m = 32 * q + lane;        // TMEM lane = D row = 2k + b
+    const int m = 32 * q + lane;  // TMEM lane = D row = 2k + b
     const int kk_ = m >> 1, bsel = m & 1;
     const uint32_t lane_off = (uint32_t)(32 * q) << 16;
 
-    float4 cur[8];
-    auto load_line = [&](long long f) {
+    uint32_t phase = 0;
+    bool aborted = false;
+    for (long long f = (long long)blockIdx.x * TQ_PIPES + p; f < batch; f += (long long)gridDim.x * TQ_PIPES) {
+        // ---- the line, its scale, the stage-1 operand (MN-major) ----
+        float4 cur[16];
         const float4* src = reinterpret_cast<const float4*>(in + (size_t)f * TC_N);
 #pragma unroll
-        for (int it = 0; it < 2; ++it)
+        for (int it = 0; it < 4; ++it)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) cur[4 * it + j] = __ldcs(src + 4 * (tid + TC_THREADS * it) + j);
-    };
-
-    // per-warp partial max of the line in `cur`, published through red1 by
-    // the barrier that precedes its use
-    auto publish_max = [&]() {
-        float mx = 0.f;
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-            mx = fmaxf(mx, fmaxf(fmaxf(fabsf(cur[i].x), fabsf(cur[i].y)), fmaxf(fabsf(cur[i].z), fabsf(cur[i].w))));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if (lane == 0) red1[warp] = mx;
-    };
-
-    uint32_t phase = 0;
-    long long f = blockIdx.x;
-    if (f < batch) {
-        load_line(f);
-        if constexpr (SPLIT) publish_max();
-    }
-    __syncthreads();
-    for (; f < batch; f += gridDim.x) {
-        // ---- stage-1 operand: scale, split, write B (MN-major) ----
+            for (int j = 0; j < 4; ++j) cur[4 * it + j] = __ldcs(src + 4 * (ptid + TQ_PT * it) + j);
         if constexpr (INV) {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
+            for (int i = 0; i < 16; ++i) {
                 cur[i].y = -cur[i].y;
                 cur[i].w = -cur[i].w;
             }
         }
         float s1 = 1.f;
         if constexpr (SPLIT) {
-            float m = red1[0];
+            float mx = 0.f;
 #pragma unroll
-            for (int w = 1; w < TC_THREADS / 32; ++w) m = fmaxf(m, red1[w]);
-            s1 = line_scale(m);
+            for (int i = 0; i < 16; ++i)
+                mx = fmaxf(mx, fmaxf(fmaxf(fabsf(cur[i].x), fabsf(cur[i].y)), fmaxf(fabsf(cur[i].z), fabsf(cur[i].w))));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            if (lane == 0) red1[p][q] = mx;
+            pipe_sync(p);
+            s1 = line_scale(fmaxf(fmaxf(red1[p][0], red1[p][1]), fmaxf(red1[p][2], red1[p][3])));
         }
 #pragma unroll
-        for (int it = 0; it < 2; ++it) {
-            const int item = tid + TC_THREADS * it;  // (n1, c): n2 = 8c .. 8c+7
+        for (int it = 0; it < 4; ++it) {
+            const int item = ptid + TQ_PT * it;  // (n1, c): n2 = 8c .. 8c+7
             const int n1 = item >> 3, c = item & 7;
             float re[8], im[8];
 #pragma unroll
@@ -265,52 +257,48 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
                 re[2 * j + 1] = v.z * s1;
                 im[2 * j + 1] = v.w * s1;
             }
-            // MN-major rows kk = 2*n1 (re) and 2*n1 + 1 (im), chunk c of n2
-            store_chunk<SPLIT>(smem, mnmaj_off(8 * c, 2 * n1), re);
-            store_chunk<SPLIT>(smem, mnmaj_off(8 * c, 2 * n1 + 1), im);
+            store_chunk_b<SPLIT>(bp, mnmaj_off(8 * c, 2 * n1), re);
+            store_chunk_b<SPLIT>(bp, mnmaj_off(8 * c, 2 * n1 + 1), im);
         }
-        // prefetch the next line: in flight during the tensor-core work
-        if (f + gridDim.x < batch) load_line(f + gridDim.x);
         fence_proxy_async_smem();
         tc::fence_before_sync();
-        __syncthreads();
+        pipe_sync(p);
 
-        // ---- stage 1 on the tensor cores ----
-        if (tid == 0) {
+        // ---- stage 1 ----
+        if (ptid == 0) {
             tc::fence_after_sync();
-            issue_product<SPLIT, true>(d1, sbase, IDESC1);
-            tc::mma_commit(&mbar);
-            if (!mbar_wait(&mbar, phase)) abort_sh = 1;
+            issue_product_q<SPLIT, true>(d1, sbase, baddr, IDESC1);
+            tc::mma_commit(&mbar[p]);
+            if (!mbar_wait(&mbar[p], phase)) abort_sh[p] = 1;
         }
         phase ^= 1u;
-        __syncthreads();
-        if (abort_sh) break;
+        pipe_sync(p);
+        if (abort_sh[p]) {
+            aborted = true;
+            break;
+        }
         tc::fence_after_sync();
 
-        // ---- epilogue 1: unscale, pair re/im, twiddle, scale, write B (K-major) ----
-        float2 z[16];
-        {
-            float v[32];
-            tc::tmem_ld32(d1 + lane_off + 32 * h, v);
-            const float inv1 = 1.f / ((SPLIT ? TC_GSCALE : 1.f) * s1);
+        // ---- epilogue 1: unscale, pair re/im, twiddle, scale, stage-2 operand (K-major) ----
+        const float inv1 = 1.f / ((SPLIT ? TC_GSCALE : 1.f) * s1);
+        const float s2 = SPLIT ? s1 * (1.f / 64.f) : 1.f;
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+            float2 z[16];
+            {
+                float v[32];
+                tc::tmem_ld32(d1 + lane_off + 32 * h, v);
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const float send = bsel ? v[i] : v[16 + i];
-                const float r = __shfl_xor_sync(0xffffffffu, send, 1);
-                z[i] = bsel ? make_float2(r * inv1, v[16 + i] * inv1) : make_float2(v[i] * inv1, r * inv1);
+                for (int i = 0; i < 16; ++i) {
+                    const float send = bsel ? v[i] : v[16 + i];
+                    const float r = __shfl_xor_sync(0xffffffffu, send, 1);
+                    z[i] = bsel ? make_float2(r * inv1, v[16 + i] * inv1) : make_float2(v[i] * inv1, r * inv1);
+                }
             }
-        }
-        const int n2_0 = 32 * h + 16 * bsel;  // this thread's n2 range; k1 = kk_
-        {
+            const int n2_0 = 32 * h + 16 * bsel;
             const float2 w0 = t0[(n2_0 >> 4) * 64 + kk_];
 #pragma unroll
             for (int i = 0; i < 16; ++i) z[i] = cmul(z[i], cmul(w0, t1[i * 64 + kk_]));
-        }
-        // a DFT-64 grows magnitudes by at most 64: s1 / 64 keeps |Z| s2 < 2^14
-        // without a second reduction over the line
-        const float s2 = SPLIT ? s1 * (1.f / 64.f) : 1.f;
-        {
-            // K-major row nn = k1, K = 2*n2 + a: 4 chunks of 8 (4 complex values)
 #pragma unroll
             for (int qq = 0; qq < 4; ++qq) {
                 float x[8];
@@ -319,30 +307,34 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
                     x[2 * j] = z[4 * qq + j].x * s2;
                     x[2 * j + 1] = z[4 * qq + j].y * s2;
                 }
-                store_chunk<SPLIT>(smem, kmaj_off(kk_, 2 * (n2_0 + 4 * qq), B2_KATOM), x);
+                store_chunk_b<SPLIT>(bp, kmaj_off(kk_, 2 * (n2_0 + 4 * qq), B2_KATOM), x);
             }
         }
         fence_proxy_async_smem();
         tc::fence_before_sync();
-        __syncthreads();
+        pipe_sync(p);
 
-        // ---- stage 2 on the tensor cores ----
-        if (tid == 0) {
+        // ---- stage 2 ----
+        if (ptid == 0) {
             tc::fence_after_sync();
-            issue_product<SPLIT, false>(d2, sbase, IDESC2);
-            tc::mma_commit(&mbar);
-            if (!mbar_wait(&mbar, phase)) abort_sh = 1;
+            issue_product_q<SPLIT, false>(d2, sbase, baddr, IDESC2);
+            tc::mma_commit(&mbar[p]);
+            if (!mbar_wait(&mbar[p], phase)) abort_sh[p] = 1;
         }
         phase ^= 1u;
-        __syncthreads();
-        if (abort_sh) break;
+        pipe_sync(p);
+        if (abort_sh[p]) {
+            aborted = true;
+            break;
+        }
         tc::fence_after_sync();
 
         // ---- epilogue 2: unscale, pair re/im, store X[k1 + 64 k2] ----
-        {
+        const float inv2 = (INV ? 1.f / (float)TC_N : 1.f) / ((SPLIT ? TC_GSCALE : 1.f) * s2);
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
             float v[32];
             tc::tmem_ld32(d2 + lane_off + 32 * h, v);
-            const float inv2 = (INV ? 1.f / (float)TC_N : 1.f) / ((SPLIT ? TC_GSCALE : 1.f) * s2);
             float4 o[8];
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
@@ -363,36 +355,32 @@ __global__ void __launch_bounds__(TC_THREADS, 2)
 #pragma unroll
             for (int i = 0; i < 8; ++i) __stcs(dst + i, o[i]);
         }
-        if constexpr (SPLIT) {
-            if (f + gridDim.x < batch) publish_max();  // the prefetched line
-        }
         tc::fence_before_sync();
-        __syncthreads();  // TMEM and B are free for the next line; red1 published
+        pipe_sync(p);  // this pipeline's TMEM columns and B buffers are free for its next line
     }
 
-    if (abort_sh && tid == 0) {
+    if (aborted && ptid == 0) {
         report_device_error(dev_err, DEV_ERR_MMA_TIMEOUT);
-        mbar_wait(&mbar, phase ^ 1u);  // bounded: let an MMA still in flight finish
+        mbar_wait(&mbar[p], phase ^ 1u);  // bounded: let an MMA still in flight finish
     }
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, TMEM_COLS);
+        tc::tmem_dealloc(tmem_base_sh, 512);
     }
 }
 
 template <bool SPLIT, bool INV>
-cudaError_t launch_tc(const float2* in, float2* out, long long batch, const uint4* gimg, const float2* tw,
-                      int* dev_err, int sms, cudaStream_t s) {
-    // the shared-memory opt-in is a per-device attribute: set it on the
-    // current device at every call (a few microseconds)
-    cudaError_t e = cudaFuncSetAttribute(k_fft4096_tc<SPLIT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM_BYTES);
+cudaError_t launch_tcq(const float2* in, float2* out, long long batch, const uint4* gimg, const float2* tw,
+                       int* dev_err, int sms, cudaStream_t s) {
+    cudaError_t e = cudaFuncSetAttribute(k_fft4096_tcq<SPLIT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TQ_SMEM);
     if (e != cudaSuccess) return e;
-    long long blocks = (long long)sms * 2;
-    if (blocks > batch) blocks = batch;
+    long long blocks = (batch + TQ_PIPES - 1) / TQ_PIPES;
+    if (blocks > sms) blocks = sms;
     if (blocks <= 0) return cudaSuccess;
-    k_fft4096_tc<SPLIT, INV><<<(unsigned)blocks, TC_THREADS, SM_BYTES, s>>>(in, out, batch, gimg, tw, dev_err);
+    k_fft4096_tcq<SPLIT, INV><<<(unsigned)blocks, TQ_THREADS, TQ_SMEM, s>>>(in, out, batch, gimg, tw, dev_err);
     return cudaGetLastError();
 }
 
@@ -435,11 +423,11 @@ int tc_launch(mfft_plan* p, const float2* in, float2* out, int64_t batch, int di
     cudaError_t e;
     const bool inv = (direction == MFFT_INVERSE);
     if (variant == MFFT_TC_FP16_SPLIT3)
-        e = inv ? launch_tc<true, true>(in, out, batch, g_split, p->tc.tw, err, sms, s)
-                : launch_tc<true, false>(in, out, batch, g_split, p->tc.tw, err, sms, s);
+        e = inv ? launch_tcq<true, true>(in, out, batch, g_split, p->tc.tw, err, sms, s)
+                : launch_tcq<true, false>(in, out, batch, g_split, p->tc.tw, err, sms, s);
     else
-        e = inv ? launch_tc<false, true>(in, out, batch, g_bf, p->tc.tw, err, sms, s)
-                : launch_tc<false, false>(in, out, batch, g_bf, p->tc.tw, err, sms, s);
+        e = inv ? launch_tcq<false, true>(in, out, batch, g_bf, p->tc.tw, err, sms, s)
+                : launch_tcq<false, false>(in, out, batch, g_bf, p->tc.tw, err, sms, s);
     if (e != cudaSuccess) return cuda_error(e, "tensor-core FFT launch");
     return MFFT_SUCCESS;
 }
