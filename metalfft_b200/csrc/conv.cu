@@ -521,7 +521,11 @@ extern "C" int mfft_conv_set_precision(mfft_conv* c, int precision) {
                              "FusedConvolver only supports fftSize=4096 in FP16 modes, got %lld", (long long)c->fft);
         DeviceGuard g(c->ctx->device);
         const int occ = conv_fp16_ctas_per_sm(precision);
-        if (occ <= 0) return cuda_error(cudaGetLastError(), "FP16 convolver kernel attributes");
+        if (occ <= 0) {
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return cuda_error(e, "FP16 convolver kernel attributes");
+            return set_error(MFFT_ERR_LIBRARY_BUILD, -1, -1, -1, "the FP16 convolver kernel cannot be resident on this device");
+        }
         c->fp16_occ = occ;
     }
     c->precision = precision;
