@@ -324,3 +324,29 @@ def test_host_arrays_across_staging_chunks(M, kind, n, b):
         yh = torch.empty(shape_out, dtype=dt_out, pin_memory=pinned)
         M._check(run(xs, yh, M.HOST))
         assert torch.equal(yh, ref), (kind, n, b, pinned)
+
+
+@pytest.mark.parametrize("n", [1 << 16, 1 << 17, 1 << 18, 1 << 19, 1 << 20])
+def test_tma_fourstep_inverse_odd_batch_in_place(M, n):
+    """Four-step sizes whose tiles move by TMA: forward and inverse of an odd
+    batch against FP64; in place equal to out of place; one line alone equal
+    to the same line inside the batch (bit for bit)."""
+    import torch
+    b = 3
+    x = O.normal_c64((b, n), seed=5000 + n)
+    f = M.MetalFFT(n)
+    xd = torch.from_numpy(x).cuda()
+    y = torch.empty_like(xd)
+    f.exec(xd, y, b, M.FORWARD)
+    zi = torch.empty_like(xd)
+    f.exec(xd, zi, b, M.INVERSE)
+    one = torch.empty_like(xd[1:2])
+    f.exec(xd[1:2].clone(), one, 1, M.FORWARD)
+    ip = xd.clone()
+    f.exec(ip, ip, b, M.FORWARD)
+    torch.cuda.synchronize()
+    assert M.lib.mfft_context_check(M.shared_context()) == 0
+    assert O.rel_rms(y.cpu().numpy(), O.truth(x)) < TOL_BIG
+    assert O.rel_rms(zi.cpu().numpy(), O.truth(x, inverse=True)) < TOL_BIG
+    assert torch.equal(ip, y)
+    assert torch.equal(one[0], y[1])
