@@ -166,8 +166,10 @@ __device__ __forceinline__ void do_cols(float2* st, float2* __restrict__ mid, in
     __syncthreads();  // every exchange read is done before the output tile overwrites the stage
 #pragma unroll
     for (int m = 0; m < 16; ++m) st[tidx(t + m * T, c, LC)] = v[m];
-    __syncthreads();
-    if constexpr (!TILE_OUT) store_tile<false>(st, mid + col0, LL, LC, 1LL << ln2);
+    if constexpr (!TILE_OUT) {  // (the TMA caller fences and synchronises before its bulk store)
+        __syncthreads();
+        store_tile<false>(st, mid + col0, LL, LC, 1LL << ln2);
+    }
 }
 
 template <int L, bool INV, bool TILE_OUT = false>
@@ -187,8 +189,10 @@ __device__ __forceinline__ void do_rows(float2* st, const float2* mid_rows, floa
 #pragma unroll
     for (int m = 0; m < 16; ++m)
         st[tidx(t + m * T, r, LR)] = INV ? make_float2(v[m].x * scale, -v[m].y * scale) : v[m];
-    __syncthreads();
-    if constexpr (!TILE_OUT) store_tile<true>(st, out + row0, LL, LR, 1LL << ln1);
+    if constexpr (!TILE_OUT) {
+        __syncthreads();
+        store_tile<true>(st, out + row0, LL, LR, 1LL << ln1);
+    }
 }
 
 // ---- items ----------------------------------------------------------------------
