@@ -328,7 +328,10 @@ __global__ void __launch_bounds__(XS_THREADS, 2)
         float2* dst = stage + (si & 1) * elems;
         const long long fs = fa + (long long)si * XF;
         for (int e = 2 * threadIdx.x; e < elems; e += 2 * XS_THREADS) {
-            const int fr = e / (C * KB), rem = e - fr * C * KB, c = rem / KB, bb = rem - c * KB;
+            // XF = 2 frames per stage; KB is a power of two
+            static_assert(XF == 2 && (KB & (KB - 1)) == 0, "stage index arithmetic");
+            const int fr = e >= C * KB ? 1 : 0, rem = e - fr * C * KB;
+            const int c = rem >> ilog2c(KB), bb = rem & (KB - 1);
             const long long f = fs + fr;
             const bool ok = f < fb;
             const int kk = min(tile0 + bb, nbins - 1);
