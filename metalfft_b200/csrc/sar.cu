@@ -356,31 +356,60 @@ __global__ void __launch_bounds__(NR / SAR_E) k_sar_rcmc(const __half2* __restri
     }
     __syncthreads();
     const RcmcRow R = rows[k];
+    // matched-filter phasors e^{+-j 2 pi (alpha + beta r)} of this thread's bins
+    // r = t + m*T: the phase of r = t formed in FP64 and reduced to one cycle,
+    // times products of at most three of e^{+-j 2 pi beta T {1, 2, 4, 8}}
+    float2 h[SAR_E];
+    {
+        auto phasor = [&](double cyc) {
+            const float f = (float)(cyc - floor(cyc));
+            float sn, cs;
+            sincospif(2.0f * f, &sn, &cs);
+            return R.valid ? make_float2(cs, R.sign * sn) : make_float2(0.f, 0.f);
+        };
+        const float2 base = phasor(fma((double)t, R.beta, R.alpha));
+        const double bt = R.beta * (double)T;
+        const float2 s1 = phasor(bt), s2 = phasor(2.0 * bt), s4 = phasor(4.0 * bt), s8 = phasor(8.0 * bt);
+        float2 u[4];
+        u[0] = base;
+        u[1] = cmul(base, s1);
+        u[2] = cmul(base, s2);
+        u[3] = cmul(u[1], s2);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float2 w4 = cmul(u[q], s4);
+            h[q] = u[q];
+            h[q + 4] = w4;
+            h[q + 8] = cmul(u[q], s8);
+            h[q + 12] = cmul(w4, s8);
+        }
+    }
     float2 v[SAR_E];
     float mx = 0.f;
 #pragma unroll
     for (int m = 0; m < SAR_E; ++m) {
         const int r = t + m * T;
+        const int lo = r + R.c0 - 3;  // taps lo .. lo + 7
         float2 acc = make_float2(0.f, 0.f);
+        if (lo >= 0 && lo + 7 < NR) {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int idx = r + R.c0 + j - 3;
-            if (idx >= 0 && idx < NR) {
-                const float2 x = line[idx];
+            for (int j = 0; j < 8; ++j) {
+                const float2 x = line[lo + j];
                 acc.x = fmaf(x.x, R.w[j], acc.x);
                 acc.y = fmaf(x.y, R.w[j], acc.y);
             }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int idx = lo + j;
+                if (idx >= 0 && idx < NR) {
+                    const float2 x = line[idx];
+                    acc.x = fmaf(x.x, R.w[j], acc.x);
+                    acc.y = fmaf(x.y, R.w[j], acc.y);
+                }
+            }
         }
-        float2 h = make_float2(0.f, 0.f);
-        if (R.valid) {
-            // phase in cycles in FP64, reduced to [0, 1) before the FP32 sincospi
-            const double cyc = fma((double)r, R.beta, R.alpha);
-            const float f = (float)(cyc - floor(cyc));
-            float sn, cs;
-            sincospif(2.0f * f, &sn, &cs);
-            h = make_float2(cs, R.sign * sn);
-        }
-        v[m] = cmul(acc, h);
+        v[m] = cmul(acc, h[m]);
         mx = fmaxf(mx, fmaxf(fabsf(v[m].x), fabsf(v[m].y)));
     }
     const float s = block_scale(cta_max(mx, red));
