@@ -175,6 +175,41 @@ def fp64_check(x_rows, y_rows):
     return float(np.linalg.norm(y_rows - ref) / np.linalg.norm(ref))
 
 
+def link_ceiling(hin, hout, din, dout, transforms, reps=3):
+    """The host link's ceiling for the e2e call: the same bytes copied both ways at once
+    (pinned host -> device on one stream, device -> host on another, no transform),
+    timed with CUDA events. e2e value / link_transforms_per_s is the share of the link
+    the C-ABI call reaches."""
+    import torch
+    cur = torch.cuda.current_stream()
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def both():
+        up.wait_stream(cur)
+        down.wait_stream(cur)
+        with torch.cuda.stream(up):
+            din.copy_(hin, non_blocking=True)
+        with torch.cuda.stream(down):
+            hout.copy_(dout, non_blocking=True)
+        cur.wait_stream(up)
+        cur.wait_stream(down)
+
+    both()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(cur)
+    for _ in range(reps):
+        both()
+    e1.record(cur)
+    torch.cuda.synchronize()
+    s = e0.elapsed_time(e1) / reps / 1e3
+    nbytes = hin.numel() * hin.element_size()
+    return {"link_gbs_per_direction": nbytes / s / 1e9,
+            "link_transforms_per_s": transforms / s,
+            "link_note": "plain pinned copies of the same bytes, both directions at once"}
+
+
 def cpu_baseline(seconds=12.0):
     """The reference algorithm (FP32 radix-4 Stockham, oracle/) on all host
     cores over a bounded sample of the same workload."""
@@ -722,6 +757,7 @@ def main():
     e2e = {"value": B * world * args.e2e_steps / dt, "unit": "transforms/s",
            "h2d_bytes_per_step": B * N * 8, "d2h_bytes_per_step": B * N * 8,
            "steps": args.e2e_steps}
+    e2e.update(link_ceiling(hin, hout, x, y, B * world))
 
     kernel_name = "k_fft_batched" if best == "fp32" else "k_fft4096_tcq"
     line = {

@@ -61,6 +61,11 @@ struct ConvGeom {
     static constexpr int MINB_FWD = THREADS <= 256 ? 2 : 1;
 };
 
+// number of valid samples in a window of `cap` when `avail` remain (0 .. cap)
+__device__ __forceinline__ int clamp_count(long long avail, int cap) {
+    return avail <= 0 ? 0 : (avail >= cap ? cap : (int)avail);
+}
+
 template <bool WS>
 __device__ __forceinline__ void cta_sync() {
     __syncthreads();
@@ -105,16 +110,18 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, ConvGeom<FFT>::MINB_FW
         const bool active = it < iters_mine;
         const long long p = pw + it;
         const long long b = 2 * p;
+        // 32-bit offsets from the pair's base: lim0 / lim1 = valid samples of blocks b, b+1
+        const long long base = b * hop;
+        const float* xb = x + base;
+        const int lim0 = active ? clamp_count(nx - base, hop) : 0;
+        const int lim1 = active ? clamp_count(nx - base - hop, hop) : 0;
         float2 v[CONV_E];
 #pragma unroll
         for (int m = 0; m < CONV_E; ++m) {
             const int i = t + m * T;
-            const long long s0 = b * hop + i, s1 = s0 + hop;
             float re = 0.f, im = 0.f;
-            if (active && i < hop) {
-                if (s0 < nx) re = __ldcs(x + s0);
-                if (s1 < nx) im = __ldcs(x + s1);
-            }
+            if (i < lim0) re = __ldcs(xb + i);
+            if (i < lim1) im = __ldcs(xb + hop + i);
             v[m] = make_float2(re, im);
         }
         fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
@@ -126,13 +133,15 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, ConvGeom<FFT>::MINB_FW
         fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
         // v[m] = conj(FFT * FFT) -> r = conj(v)/FFT; re = block b, im = block b+1
         const bool write = active && p >= p0;
+        float* yb = y + base;
+        const int wlim0 = write ? clamp_count(ny - base, hop) : 0;
+        const int wlim1 = write ? clamp_count(ny - base - hop, hop) : 0;
 #pragma unroll
         for (int m = 0; m < CONV_E; ++m) {
             const int i = t + m * T;
             const float val = v[m].x * sc + acc0[i];
             if (i < hop) {
-                const long long o = b * hop + i;
-                if (write && o < ny) __stcs(y + o, val);
+                if (i < wlim0) __stcs(yb + i, val);
             } else {
                 acc1[i - hop] = val;
             }
@@ -143,8 +152,7 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, ConvGeom<FFT>::MINB_FW
             const int i = t + m * T;
             const float val = -v[m].y * sc + acc1[i];
             if (i < hop) {
-                const long long o = (b + 1) * hop + i;
-                if (write && o < ny) __stcs(y + o, val);
+                if (i < wlim1) __stcs(yb + hop + i, val);
             } else {
                 acc0[i - hop] = val;
             }
@@ -188,16 +196,18 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
         for (int q = 0; q < 2; ++q) {
             const long long b = b0 + it + q;
             const bool active = (it + q) < mine;
+            const long long base = b * hop;
+            const int glim = active ? clamp_count(ny - base, FFT) : 0;
+            const int xlim = active ? clamp_count(nx - base, hop) : 0;
+            const float* gb = g + base;
+            const float* xb = x + base;
             float2 v[CONV_E];
 #pragma unroll
             for (int m = 0; m < CONV_E; ++m) {
                 const int i = t + m * T;
-                const long long gi = b * hop + i;
                 float re = 0.f, im = 0.f;
-                if (active) {
-                    if (gi < ny) re = __ldcs(g + gi);
-                    if (i < hop && gi < nx) im = __ldcs(x + gi);
-                }
+                if (i < glim) re = __ldcs(gb + i);
+                if (i < xlim) im = __ldcs(xb + i);
                 v[m] = make_float2(re, im);
             }
             fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
@@ -229,15 +239,15 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
         fft_regs<FFT, CONV_E, G::WS>(S, t, buf, tw);
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const long long b = b0 + it + q;
-            if ((it + q) >= mine) continue;
+            const long long base = (b0 + it + q) * hop;
+            const int lim = (it + q) < mine ? clamp_count(nx - base, hop) : 0;
+            float* db = dx + base;
 #pragma unroll
             for (int m = 0; m < CONV_E; ++m) {
                 const int i = t + m * T;
-                const long long o = b * hop + i;
                 // r = conj(S)/FFT: re = block b, im = block b+1
                 const float val = (q == 0 ? S[m].x : -S[m].y) * sc;
-                if (i < hop && o < nx) __stcs(dx + o, val);
+                if (i < lim) __stcs(db + i, val);
             }
         }
     }
