@@ -175,6 +175,11 @@ def fp64_check(x_rows, y_rows):
     return float(np.linalg.norm(y_rows - ref) / np.linalg.norm(ref))
 
 
+def fft_flops(n):
+    """The conventional FFT operation count of one complex n-point transform, 5 n log2 n."""
+    return 5.0 * n * (n.bit_length() - 1)
+
+
 def link_ceiling(hin, hout, din, dout, transforms, reps=3):
     """The host link's ceiling for the e2e call: the same bytes copied both ways at once
     (pinned host -> device on one stream, device -> host on another, no transform),
@@ -338,6 +343,7 @@ def run_reference(args, rank, world):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "gflop_per_s": v * fft_flops(N) / 1e9, "gflop_note": "5 N log2 N per transform",
         "config": {"workload": "batched C2C FFT N=4096, complex64 N(0,1) seeded; each step a "
                                "bounded sample of %d of the 16384 lines" % sample,
                    "n": N, "batch": sample},
@@ -405,6 +411,8 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
         line.update({"metric": "batched C2C FFT N=4096 x 256: transforms/s (forward + inverse)",
                      "value": 2 * b * world * args.steps / (ms_max / 1e3), "unit": "transforms/s",
                      "ms_per_step": ms_max / args.steps, "rel_rms": err,
+                     "gflop_per_s": 2 * b * world * args.steps / (ms_max / 1e3) * fft_flops(n) / 1e9,
+                     "gflop_note": "5 N log2 N per transform",
                      "config": {"workload": "C2C FFT N=4096 x 256 lines, U[-1,1) seeded, forward then inverse",
                                 "l2": "64 rotating buffer sets (1 GiB) > L2",
                                 "graph": "one CUDA graph per step (forward + inverse launch)"},
@@ -424,6 +432,9 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
         line.update({"metric": "mixed-size FFT batch on the persistent item kernel: points/s",
                      "value": mb.points * world * args.steps / (ms_max / 1e3), "unit": "points/s",
                      "ms_per_step": ms_max / args.steps, "transforms_per_step": ntr,
+                     "gflop_per_s": sum(c * fft_flops(n) for n, c in classes) * world * args.steps
+                     / (ms_max / 1e3) / 1e9,
+                     "gflop_note": "5 N log2 N per transform, summed over the classes",
                      "config": {"workload": "sizes 2^6..2^14 + 2^20, counts U{1..512} seeded, <= 2^26 points",
                                 "classes": classes, "points": mb.points,
                                 "graph": "one CUDA graph per step: four launches of the item kernel"},
@@ -721,6 +732,7 @@ def main():
         gbs = BYTES_PER_TRANSFORM * B / per_launch_s / 1e9
         results[name] = {
             "transforms_per_s": B * world * args.steps / (ms_max / 1e3),
+            "gflop_per_s": B * world * args.steps / (ms_max / 1e3) * fft_flops(N) / 1e9,
             "ms_per_step": ms_max / args.steps,
             "rel_rms": err,
             "hbm_gbs": gbs,
@@ -778,6 +790,8 @@ def main():
                    "n": N, "batch_per_gpu": B, "variant": best, "parallelism": "replicas",
                    "l2": "inputs larger than L2 (%d MiB read + %d MiB written per step)" % (B // 32, B // 32)},
         "rel_rms": r["rel_rms"],
+        "gflop_per_s": r["gflop_per_s"],
+        "gflop_note": "5 N log2 N per transform",
         "variants": results,
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": r["hbm_gbs"], "peak": peak, "unit": "GB/s",
