@@ -350,3 +350,47 @@ def test_tma_fourstep_inverse_odd_batch_in_place(M, n):
     assert O.rel_rms(zi.cpu().numpy(), O.truth(x, inverse=True)) < TOL_BIG
     assert torch.equal(ip, y)
     assert torch.equal(one[0], y[1])
+
+
+def test_plans_of_the_shared_context_on_concurrent_threads(M):
+    # MetalContext.shared is one lock-protected context used by every MetalFFT
+    # instance (MetalContext.swift:79-88); each instance is single-threaded
+    # (MetalFFT.swift:9).  Here four threads, each with its own plans on the
+    # shared context, run host-array calls at the same time (ctypes releases
+    # the GIL during each call): the staged chunk pipeline, the single-chunk
+    # path, a four-step plan and the tensor-core kernel overlap.  Every result
+    # matches FP64 and repeats bitwise.
+    import threading
+    jobs = [("c2c-chunks", 4096, 1024, 0), ("c2c-small", 1024, 64, 0),
+            ("fourstep", 1 << 16, 8, 0), ("tc-split", 4096, 512, M.TC_FP16_SPLIT3)]
+    errors, results = [], {}
+
+    def work(name, n, b, tc, seed):
+        try:
+            f = M.MetalFFT(n)
+            rng = np.random.default_rng(seed)
+            x = (rng.standard_normal((b, n)) + 1j * rng.standard_normal((b, n))).astype(np.complex64)
+            first = None
+            for _ in range(4):
+                y = f.forward_batch(x, tc_variant=tc)
+                if first is None:
+                    first = y.copy()
+                elif not np.array_equal(y, first):
+                    errors.append("%s: a repeated call differs" % name)
+            results[name] = (x, first)
+        except Exception as e:  # noqa: BLE001 -- reported below
+            errors.append("%s: %r" % (name, e))
+
+    threads = [threading.Thread(target=work, args=(name, n, b, tc, 100 + i))
+               for i, (name, n, b, tc) in enumerate(jobs)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=300)
+    assert not any(t.is_alive() for t in threads)
+    assert not errors, errors
+    for name, n, b, tc in jobs:
+        x, y = results[name]
+        ref = np.fft.fft(x.astype(np.complex128), axis=-1)
+        err = float(np.linalg.norm(y - ref) / np.linalg.norm(ref))
+        assert err <= (3e-6 if tc or n > 16384 else 2e-6), (name, err)
