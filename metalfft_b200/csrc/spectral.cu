@@ -31,7 +31,11 @@
 //    warp groups split the upper-triangle channel pairs, with the pair sums in
 //    registers and the channel values of a few frames staged in shared memory
 //    by cp.async; the sums of each frame slice carry over from chunk to chunk
-//    in a fixed order;
+//    in a fixed order.  For 2, 4 and 8 channels the channel count is a
+//    compile-time constant: each thread loads a bin's C values and powers
+//    into registers once per frame and forms its pairs from them with static
+//    indices; other counts read each pair's two values through a table of
+//    byte offsets;
 //  * k_xspec_finish sums the slices in FP64, divides by the frame count and
 //    mirrors bins n/2+1 .. n-1 from their conjugates.
 #include <vector>
@@ -258,8 +262,9 @@ __global__ void __launch_bounds__(SpGeom<FFT>::THREADS)
 
 // k_xspec_acc geometry: G warp groups split the pairs; KB = XS_THREADS / G
 // bins per CTA; up to XQ pairs and xs_pmax(G) channel powers per thread; XF
-// frames per stage, two stages in flight.
-constexpr int XS_THREADS = 512, XQ = 8, XF = 2, XS_MAX_CH = 16, XS_MAX_G = 16;
+// frames per stage, XS_ST stage buffers (XS_ST - 1 stages in flight while one
+// is summed; <= 98 KB per CTA at any channel count, two CTAs per SM).
+constexpr int XS_THREADS = 512, XQ = 8, XF = 2, XS_ST = 3, XS_MAX_CH = 16, XS_MAX_G = 16;
 constexpr int XS_MAX_PAIRS = XS_MAX_CH * (XS_MAX_CH - 1) / 2;
 // largest channel count with ceil(P / G) <= XQ, divided over G groups
 __host__ __device__ constexpr int xs_pmax(int g) { return g == 1 ? 4 : g == 2 ? 3 : g <= 8 ? 2 : 1; }
@@ -270,14 +275,17 @@ inline int xs_groups(int C) {
         if ((P + g - 1) / g <= XQ) return g;
     return XS_MAX_G;
 }
-inline int xs_smem(int C, int g) { return 2 * XF * C * (XS_THREADS / g) * (int)sizeof(float2); }
+inline int xs_smem(int C, int g) { return XS_ST * XF * C * (XS_THREADS / g) * (int)sizeof(float2); }
 
 __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool valid) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gsrc), "r"(valid ? 16 : 0) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit_xs() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1_xs() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+// all but the XS_ST - 1 most recent copy groups have landed
+__device__ __forceinline__ void cp_async_wait_xs() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(XS_ST - 1) : "memory");
+}
 // 1/x within one unit in the last place (PTX rcp.approx.f32)
 __device__ __forceinline__ float rcp_approx(float x) {
     float r;
@@ -285,16 +293,82 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return r;
 }
 
+// Upper-triangle pair q of C channels: (xs_pi, xs_pj), row i holding the
+// C - 1 - i pairs (i, i+1) .. (i, C-1) (fft_cross_spectral.metal:51-61 order).
+__host__ __device__ constexpr int xs_pi(int C, int q) {
+    int i = 0;
+    while (q >= C - 1 - i) q -= C - 1 - i++;
+    return i;
+}
+__host__ __device__ constexpr int xs_pj(int C, int q) {
+    int i = 0;
+    while (q >= C - 1 - i) q -= C - 1 - i++;
+    return i + 1 + q;
+}
+
+// One frame of one bin for warp group GI when the channel count C is a
+// compile-time constant: the C channel values and powers sit in registers
+// (loaded and squared once per bin and frame, as the reference's kernel does),
+// and every pair of the group reads them with static indices.
+template <int C, int G, int GI, bool COH, int Q, int QEND>
+struct XsPairs {
+    static __device__ __forceinline__ void run(const float2 (&u)[C], const float (&p)[C], float (&cr)[XQ],
+                                               float (&ci)[XQ], float (&ch)[XQ]) {
+        if constexpr (Q < QEND) {
+            constexpr int P = C * (C - 1) / 2, q0 = GI * ((P + G - 1) / G);
+            constexpr int i = xs_pi(C, q0 + Q), j = xs_pj(C, q0 + Q);
+            // S_ij = X_i conj(X_j) (fft_cross_spectral.metal:57-58)
+            const float sr = u[i].x * u[j].x + u[i].y * u[j].y;
+            const float sim = u[i].y * u[j].x - u[i].x * u[j].y;
+            cr[Q] += sr;
+            ci[Q] += sim;
+            if constexpr (COH) ch[Q] += (sr * sr + sim * sim) * rcp_approx(fmaxf(p[i] * p[j], 1e-30f));
+            XsPairs<C, G, GI, COH, Q + 1, QEND>::run(u, p, cr, ci, ch);
+        }
+    }
+};
+
+template <int C, int G, int GI, bool COH>
+__device__ __forceinline__ void xs_frame_static(const float2* U, int KB, float (&pw)[xs_pmax(G)], float (&cr)[XQ],
+                                                float (&ci)[XQ], float (&ch)[XQ]) {
+    constexpr int P = C * (C - 1) / 2, QPER = (P + G - 1) / G;
+    constexpr int Q0 = GI * QPER < P ? GI * QPER : P;
+    constexpr int QN = (Q0 + QPER < P ? Q0 + QPER : P) - Q0;
+    float2 u[C];
+    float p[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        u[c] = U[c * KB];
+        p[c] = u[c].x * u[c].x + u[c].y * u[c].y;
+    }
+#pragma unroll
+    for (int r = 0; r < xs_pmax(G); ++r)
+        if constexpr (GI < C) {
+            if (GI + G * r < C) pw[r] += p[(GI + G * r) < C ? GI + G * r : 0];
+        }
+    XsPairs<C, G, GI, COH, 0, QN>::run(u, p, cr, ci, ch);
+}
+
+template <int C, int G, bool COH, int GI = 0>
+__device__ __forceinline__ void xs_frame_dispatch(int g, const float2* U, int KB, float (&pw)[xs_pmax(G)],
+                                                  float (&cr)[XQ], float (&ci)[XQ], float (&ch)[XQ]) {
+    if constexpr (GI < G) {
+        if (g == GI) xs_frame_static<C, G, GI, COH>(U, KB, pw, cr, ci, ch);
+        else xs_frame_dispatch<C, G, COH, GI + 1>(g, U, KB, pw, cr, ci, ch);
+    }
+}
+
 // CTA (blockIdx.x = bin tile, blockIdx.y = frame slice s) of one chunk of nf
 // frames.  part[(s * planes + plane) * nbins + k], planes: C powers, then
 // Re and Im of the P cross sums (interleaved per pair), then P per-frame
 // coherence sums (only when COH).  first: store, else add.
-template <int G, bool COH>
+template <int G, bool COH, int CC = 0>
 __global__ void __launch_bounds__(XS_THREADS, 2)
     k_xspec_acc(const float2* __restrict__ X, int C, int nbins, long long nf, int per, int first,
                 float* __restrict__ part) {
+    // CC > 0: the channel count is the compile-time CC (== C)
     constexpr int KB = XS_THREADS / G, PMAX = xs_pmax(G);
-    extern __shared__ __align__(16) float2 stage[];  // [2][XF][C][KB]
+    extern __shared__ __align__(16) float2 stage[];  // [XS_ST][XF][C][KB]
     // byte offsets (channel i, channel j) of every pair inside a frame's
     // [C][KB] block, upper-triangle order (row i holds C - 1 - i pairs)
     __shared__ uint2 pair_off[XS_MAX_PAIRS];
@@ -325,29 +399,41 @@ __global__ void __launch_bounds__(XS_THREADS, 2)
     // 16-byte copies of bin pairs (KB, tile0 and nbins - 1 = n/2 are even, so a
     // pair never crosses a row's n/2 + 16 entries)
     auto issue = [&](int si) {
-        float2* dst = stage + (si & 1) * elems;
+        float2* dst = stage + (si % XS_ST) * elems;
         const long long fs = fa + (long long)si * XF;
+        // stage row r = e / KB is frame fs + r / C, channel r % C: global
+        // row fs * C + r of the chunk's [frame][channel] spectra
+        static_assert((KB & (KB - 1)) == 0, "stage index arithmetic");
+        const long long rows_left = (fb - fs) * C;
+        const float2* Xs = X + fs * C * hs;
         for (int e = 2 * threadIdx.x; e < elems; e += 2 * XS_THREADS) {
-            // XF = 2 frames per stage; KB is a power of two
-            static_assert(XF == 2 && (KB & (KB - 1)) == 0, "stage index arithmetic");
-            const int fr = e >= C * KB ? 1 : 0, rem = e - fr * C * KB;
-            const int c = rem >> ilog2c(KB), bb = rem & (KB - 1);
-            const long long f = fs + fr;
-            const bool ok = f < fb;
+            const int r = e >> ilog2c(KB), bb = e & (KB - 1);
+            const bool ok = r < rows_left;
             const int kk = min(tile0 + bb, nbins - 1);
-            cp_async16(dst + e, ok ? X + (f * C + c) * hs + kk : X, ok);
+            cp_async16(dst + e, ok ? Xs + (long long)r * hs + kk : X, ok);
         }
     };
-    if (nst > 0) issue(0);
-    cp_async_commit_xs();
+    // XS_ST - 1 stages in flight ahead of the one being summed
+#pragma unroll
+    for (int s0 = 0; s0 < XS_ST - 1; ++s0) {
+        if (s0 < nst) issue(s0);
+        cp_async_commit_xs();
+    }
     __syncthreads();  // pair_off
     for (int si = 0; si < nst; ++si) {
-        if (si + 1 < nst) issue(si + 1);
+        // refills the buffer summed in the previous iteration (all threads
+        // passed its closing barrier)
+        if (si + XS_ST - 1 < nst) issue(si + XS_ST - 1);
         cp_async_commit_xs();
-        cp_async_wait1_xs();
+        cp_async_wait_xs();
         __syncthreads();
-        if (live) {
-            const char* U0 = reinterpret_cast<const char*>(stage + (si & 1) * elems + b);
+        if (CC > 0 && live) {
+#pragma unroll
+            for (int fr = 0; fr < XF; ++fr)
+                xs_frame_dispatch<(CC > 0 ? CC : 2), G, COH>(g, stage + (si % XS_ST) * elems + fr * CC * KB + b, KB, pw,
+                                                            cr, ci, ch);
+        } else if (live) {
+            const char* U0 = reinterpret_cast<const char*>(stage + (si % XS_ST) * elems + b);
 #pragma unroll
             for (int fr = 0; fr < XF; ++fr) {
                 const char* U = U0 + fr * C * KB * 8;
@@ -511,13 +597,20 @@ const SpKernels* find_spk(int fft) {
     return nullptr;
 }
 
-template <int G, bool COH>
+template <int G, bool COH, int CC = 0>
 void xs_launch(dim3 grid, int smem, cudaStream_t s, const float2* X, int C, int nbins, long long nf, int per,
                int first, float* part) {
-    k_xspec_acc<G, COH><<<grid, XS_THREADS, smem, s>>>(X, C, nbins, nf, per, first, part);
+    k_xspec_acc<G, COH, CC><<<grid, XS_THREADS, smem, s>>>(X, C, nbins, nf, per, first, part);
 }
 using XsFn = void (*)(dim3, int, cudaStream_t, const float2*, int, int, long long, int, int, float*);
-XsFn xs_fn(int g, bool coh) {
+// channel counts 2, 4 and 8 have a compile-time kernel (G = xs_groups(C))
+XsFn xs_fn(int g, bool coh, int C) {
+    switch (C) {  // g == xs_groups(C): 1, 1, 4
+        case 2: return coh ? &xs_launch<1, true, 2> : &xs_launch<1, false, 2>;
+        case 4: return coh ? &xs_launch<1, true, 4> : &xs_launch<1, false, 4>;
+        case 8: return coh ? &xs_launch<4, true, 8> : &xs_launch<4, false, 8>;
+        default: break;
+    }
     switch (g) {
         case 1: return coh ? &xs_launch<1, true> : &xs_launch<1, false>;
         case 2: return coh ? &xs_launch<2, true> : &xs_launch<2, false>;
@@ -528,15 +621,22 @@ XsFn xs_fn(int g, bool coh) {
 }
 // shared-memory opt-in on the current device, then the resident CTAs per SM
 // (0 when the opt-in fails)
-template <int G, bool COH>
+template <int G, bool COH, int CC = 0>
 int xs_occ_of(int smem) {
-    if (cudaFuncSetAttribute(k_xspec_acc<G, COH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_xspec_acc<G, COH, CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
         return 0;
     int occ = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xspec_acc<G, COH>, XS_THREADS, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xspec_acc<G, COH, CC>, XS_THREADS, smem);
     return (e == cudaSuccess && occ > 0) ? occ : 1;
 }
-int xs_occ(int g, bool coh, int smem) {
+int xs_occ(int g, bool coh, int smem, int C) {
+    switch (C) {
+        case 2: return coh ? xs_occ_of<1, true, 2>(smem) : xs_occ_of<1, false, 2>(smem);
+        case 4: return coh ? xs_occ_of<1, true, 4>(smem) : xs_occ_of<1, false, 4>(smem);
+        case 8: return coh ? xs_occ_of<4, true, 8>(smem) : xs_occ_of<4, false, 8>(smem);
+        default: break;
+    }
     switch (g) {
         case 1: return coh ? xs_occ_of<1, true>(smem) : xs_occ_of<1, false>(smem);
         case 2: return coh ? xs_occ_of<2, true>(smem) : xs_occ_of<2, false>(smem);
@@ -845,7 +945,7 @@ int xspec_device(mfft_spectral* s, const float* x, int C, long long len, float* 
     fch = fch < 2 ? 2 : fch & ~1LL;
     if (fch > frames + (frames & 1)) fch = frames + (frames & 1);
     // frame slices: enough CTAs to fill the GPU once over the bin tiles
-    const int occ = xs_occ(g, per_frame, smem);
+    const int occ = xs_occ(g, per_frame, smem, C);
     if (!occ) return cuda_error(cudaGetLastError(), "cross-spectral kernel attributes");
     long long slices = ((long long)s->ctx->sms * occ + tiles - 1) / tiles;
     const long long max_slices = (fch + XF - 1) / XF;
@@ -859,7 +959,7 @@ int xspec_device(mfft_spectral* s, const float* x, int C, long long len, float* 
     if (!rc) rc = grow((void**)&s->xs_part, s->xs_part_floats, slices * planes * nbins, sizeof(float),
                        "cross-spectral sums");
     if (rc) return rc;
-    const XsFn acc = xs_fn(g, per_frame);
+    const XsFn acc = xs_fn(g, per_frame, C);
     for (long long f0 = 0; f0 < frames; f0 += fch) {
         const long long nf = frames - f0 < fch ? frames - f0 : fch;
         const long long lines = (long long)C * ((nf + 1) / 2);
