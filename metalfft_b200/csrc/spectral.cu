@@ -25,8 +25,9 @@
 // sums.  Here the frames go through in chunks small enough for their spectra
 // to stay in L2:
 //  * k_xstft transforms frame pairs of every channel of the chunk (the same
-//    two-real-frames-per-line split) and keeps bins 0 .. n/2 only (real
-//    input: X_{n-k} = conj X_k);
+//    two-real-frames-per-line split) and keeps bins 0 .. n/2 - 1 (real
+//    input: X_{n-k} = conj X_k); the real Nyquist bin of every frame goes to
+//    a side array for the whole call, summed by k_xspec_nyq;
 //  * k_xspec_acc owns a tile of bins and a slice of the chunk's frames; its
 //    warp groups split the upper-triangle channel pairs, with the pair sums in
 //    registers and the channel values of a few frames staged in shared memory
@@ -231,7 +232,8 @@ __host__ __device__ constexpr int xs_stride(int fft) { return fft / 2 + 16; }
 template <int FFT>
 __global__ void __launch_bounds__(SpGeom<FFT>::THREADS)
     k_xstft(const float* __restrict__ x, long long len, int C, long long f0, long long nf, int hop,
-            const float* __restrict__ win, const float2* __restrict__ tw, float2* __restrict__ X) {
+            const float* __restrict__ win, const float2* __restrict__ tw, float2* __restrict__ X,
+            float* __restrict__ nyq) {
     using G = SpGeom<FFT>;
     constexpr int T = G::T, HS = xs_stride(FFT);
     extern __shared__ __align__(16) float2 smem[];
@@ -251,9 +253,16 @@ __global__ void __launch_bounds__(SpGeom<FFT>::THREADS)
     const bool ok0 = line_ok && 2 * p < nf, ok1 = line_ok && 2 * p + 1 < nf;
     float2* r0 = X + (2 * p * C + c) * HS;
     float2* r1 = r0 + (long long)C * HS;
+    // bins 0 .. n/2 - 1 to the chunk's spectra; the Nyquist bin (real for a
+    // real frame: A and B at k = n/2 have zero imaginary parts) to nyq[frame][channel]
+    // of the whole call
+    float* nq = nyq + (f0 + 2 * p) * C + c;
     hermitian_split<FFT, G::WS>(v, t, buf, [&](int m, float2 A, float2 B) {
         const int k = t + m * T;
-        if (k <= FFT / 2) {
+        if (k == FFT / 2) {
+            if (ok0) nq[0] = A.x;
+            if (ok1) nq[C] = B.x;
+        } else if (k < FFT / 2) {
             if (ok0) r0[k] = A;
             if (ok1) r1[k] = B;
         }
@@ -375,7 +384,7 @@ __global__ void __launch_bounds__(XS_THREADS, 2)
     const int g = threadIdx.x / KB, b = threadIdx.x % KB;
     const int hs = xs_stride(2 * (nbins - 1));
     const int k = blockIdx.x * KB + b;
-    const bool live = k < nbins;
+    const bool live = k < nbins - 1;  // the Nyquist bin n/2 goes through k_xspec_nyq
     const int P = C * (C - 1) / 2;
     const int qper = (P + G - 1) / G;
     const int q0 = min(P, g * qper), qn = min(P, q0 + qper) - q0;
@@ -482,13 +491,51 @@ __global__ void __launch_bounds__(XS_THREADS, 2)
         }
 }
 
+// The Nyquist bin n/2 of every frame of the call (real values nyq[frame][channel]):
+// one CTA per item -- items 0 .. C-1 powers sum x_c^2, C .. C+P-1 pair cross
+// sums sum x_i x_j, C+P .. C+2P-1 (COH) per-frame coherence sums with the
+// pair kernel's FP32 formula.  FP64 sums, each thread over frames t, t+256,
+// ..., then a fixed-order tree: deterministic.  Launched with C + P items
+// (Welch estimate) or C + 2P (per-frame coherence).
+__global__ void __launch_bounds__(256) k_xspec_nyq(const float* __restrict__ nyq, int C, long long frames,
+                                                   double* __restrict__ out) {
+    const int P = C * (C - 1) / 2, item = blockIdx.x;
+    int i = 0, j = 0, kind = 0;  // 0 power, 1 cross, 2 coherence
+    if (item < C) {
+        i = j = item;
+    } else {
+        int r = (item - C) % P;
+        kind = item < C + P ? 1 : 2;
+        while (r >= C - 1 - i) r -= C - 1 - i++;
+        j = i + 1 + r;
+    }
+    double acc = 0.0;
+    for (long long f = threadIdx.x; f < frames; f += 256) {
+        const float xi = nyq[f * C + i], xj = nyq[f * C + j];
+        const float sr = xi * xj;
+        if (kind == 2)
+            acc += (double)((sr * sr) * rcp_approx(fmaxf((xi * xi) * (xj * xj), 1e-30f)));
+        else
+            acc += (double)sr;
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[item] = red[0];
+}
+
 // one thread per (bin k <= n/2, item): items 0 .. C-1 are powers, C .. C+P-1
 // pairs.  Fixed-order FP64 sums over the frame slices, / frames, mirrored to n - k.
 // COH: coherence = mean of the per-frame values; else the Welch estimate
 // |sum S_ij|^2 / (sum p_i sum p_j) (0 where the denominator is not positive).
 template <bool COH>
-__global__ void k_xspec_finish(const float* __restrict__ part, int slices, int C, int nbins, long long frames,
-                               float* __restrict__ power, float2* __restrict__ cross, float* __restrict__ coh) {
+__global__ void k_xspec_finish(const float* __restrict__ part, const double* __restrict__ nyq_sum, int slices, int C,
+                               int nbins, long long frames, float* __restrict__ power, float2* __restrict__ cross,
+                               float* __restrict__ coh) {
     const int P = C * (C - 1) / 2;
     const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= (long long)(C + P) * nbins) return;
@@ -496,7 +543,16 @@ __global__ void k_xspec_finish(const float* __restrict__ part, int slices, int C
     const int n = 2 * (nbins - 1);
     const int planes = C + (COH ? 3 : 2) * P;
     const double inv = 1.0 / (double)frames;
+    // the Nyquist bin's totals come from k_xspec_nyq: C powers, P cross
+    // sums (real), P coherence sums
+    const bool nyqk = k == nbins - 1;
     auto sum = [&](int plane) {
+        if (nyqk) {
+            if (plane < C) return nyq_sum[plane];
+            const int r = plane - C;
+            if (r < 2 * P) return (r & 1) ? 0.0 : nyq_sum[C + r / 2];
+            return nyq_sum[C + P + (r - 2 * P)];
+        }
         double s = 0.0;
         for (int u = 0; u < slices; ++u) s += part[((long long)u * planes + plane) * nbins + k];
         return s;
@@ -536,7 +592,7 @@ struct SpKernels {
                 long long, long long, float*);
     int (*acc_ctas_per_sm)(bool);
     void (*xstft)(dim3, cudaStream_t, const float*, long long, int, long long, long long, int, const float*,
-                  const float2*, float2*);
+                  const float2*, float2*, float*);
 };
 
 template <int FFT>
@@ -553,8 +609,8 @@ cudaError_t sp_prepare() {
 }
 template <int FFT>
 void sp_xstft(dim3 grid, cudaStream_t s, const float* x, long long len, int C, long long f0, long long nf, int hop,
-              const float* w, const float2* tw, float2* X) {
-    k_xstft<FFT><<<grid, SpGeom<FFT>::THREADS, SpGeom<FFT>::XCH * 8, s>>>(x, len, C, f0, nf, hop, w, tw, X);
+              const float* w, const float2* tw, float2* X, float* nyq) {
+    k_xstft<FFT><<<grid, SpGeom<FFT>::THREADS, SpGeom<FFT>::XCH * 8, s>>>(x, len, C, f0, nf, hop, w, tw, X, nyq);
 }
 template <int FFT>
 void sp_stft(dim3 grid, cudaStream_t s, const float* x, long long frames, int hop, const float* w, const float2* tw,
@@ -670,6 +726,10 @@ struct mfft_spectral {
     long long xs_spec_elems = 0;
     float* xs_part = nullptr;         // cross-spectral: sums per frame slice
     long long xs_part_floats = 0;
+    float* xs_nyq = nullptr;          // cross-spectral: Nyquist bin of every frame and channel
+    long long xs_nyq_floats = 0;
+    double* xs_nyq_sum = nullptr;     // cross-spectral: the Nyquist bin's totals
+    long long xs_nyq_sums = 0;
 };
 
 extern "C" int mfft_spectral_destroy(mfft_spectral* s) {
@@ -679,6 +739,8 @@ extern "C" int mfft_spectral_destroy(mfft_spectral* s) {
     cudaFree(s->part);
     cudaFree(s->xs_spec);
     cudaFree(s->xs_part);
+    cudaFree(s->xs_nyq);
+    cudaFree(s->xs_nyq_sum);
     delete s;
     return MFFT_SUCCESS;
 }
@@ -939,7 +1001,7 @@ int xspec_device(mfft_spectral* s, const float* x, int C, long long len, float* 
     const int g = xs_groups(C), kb = XS_THREADS / g, smem = xs_smem(C, g);
     if ((C + g - 1) / g > xs_pmax(g) || (P + g - 1) / g > XQ)
         return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, C, -1, "channel split %d does not fit", g);
-    const int tiles = (nbins + kb - 1) / kb;
+    const int tiles = (nbins - 1 + kb - 1) / kb;  // bins 0 .. n/2 - 1; n/2 by k_xspec_nyq
     // frames per chunk: even, at most XS_CHUNK_BYTES of spectra, no more than needed
     long long fch = XS_CHUNK_BYTES / ((long long)C * hs * 8);
     fch = fch < 2 ? 2 : fch & ~1LL;
@@ -958,23 +1020,29 @@ int xspec_device(mfft_spectral* s, const float* x, int C, long long len, float* 
     int rc = grow((void**)&s->xs_spec, s->xs_spec_elems, fch * C * hs, sizeof(float2), "cross-spectral spectra");
     if (!rc) rc = grow((void**)&s->xs_part, s->xs_part_floats, slices * planes * nbins, sizeof(float),
                        "cross-spectral sums");
+    if (!rc) rc = grow((void**)&s->xs_nyq, s->xs_nyq_floats, (frames + 1) * C, sizeof(float),
+                       "cross-spectral Nyquist bins");
+    if (!rc) rc = grow((void**)&s->xs_nyq_sum, s->xs_nyq_sums, C + 2 * P, sizeof(double),
+                       "cross-spectral Nyquist sums");
     if (rc) return rc;
     const XsFn acc = xs_fn(g, per_frame, C);
     for (long long f0 = 0; f0 < frames; f0 += fch) {
         const long long nf = frames - f0 < fch ? frames - f0 : fch;
         const long long lines = (long long)C * ((nf + 1) / 2);
         const long long ctas = (lines + s->k->lines - 1) / s->k->lines;
-        s->k->xstft(dim3((unsigned)ctas), st, x, len, C, f0, nf, (int)s->hop, s->window, s->tw, s->xs_spec);
+        s->k->xstft(dim3((unsigned)ctas), st, x, len, C, f0, nf, (int)s->hop, s->window, s->tw, s->xs_spec,
+                    s->xs_nyq);
         acc(dim3((unsigned)tiles, (unsigned)slices), smem, st, s->xs_spec, C, nbins, nf, (int)per, f0 == 0,
             s->xs_part);
     }
+    k_xspec_nyq<<<(unsigned)(C + (per_frame ? 2 : 1) * P), 256, 0, st>>>(s->xs_nyq, C, frames, s->xs_nyq_sum);
     const long long items = (long long)(C + P) * nbins;
     if (per_frame)
-        k_xspec_finish<true><<<(unsigned)((items + 255) / 256), 256, 0, st>>>(s->xs_part, (int)slices, C, nbins,
-                                                                             frames, power, cross, coh);
+        k_xspec_finish<true><<<(unsigned)((items + 255) / 256), 256, 0, st>>>(
+            s->xs_part, s->xs_nyq_sum, (int)slices, C, nbins, frames, power, cross, coh);
     else
-        k_xspec_finish<false><<<(unsigned)((items + 255) / 256), 256, 0, st>>>(s->xs_part, (int)slices, C, nbins,
-                                                                              frames, power, cross, coh);
+        k_xspec_finish<false><<<(unsigned)((items + 255) / 256), 256, 0, st>>>(
+            s->xs_part, s->xs_nyq_sum, (int)slices, C, nbins, frames, power, cross, coh);
     e = cudaGetLastError();
     return e == cudaSuccess ? MFFT_SUCCESS : cuda_error(e, "cross-spectral launch");
 }
