@@ -180,18 +180,35 @@ __global__ void __launch_bounds__(SpGeom<FFT>::THREADS, SpGeom<FFT>::MINB)
             load_pair<FFT>(a, active ? frames : 0, hop, i, t, w, v);
         }
         fft_regs<FFT, SP_E, G::WS>(v, t, buf, tw);
-        hermitian_split<FFT, G::WS>(v, t, buf, [&](int m, float2 A, float2 B) {
-            const int k = t + m * T;
-            const float pa = A.x * A.x + A.y * A.y, pb = B.x * B.x + B.y * B.y;
-            if constexpr (COH) {
-                acc[k] += pa;
-                acc[FFT + k] += pb;
+        if constexpr (COH) {
+            hermitian_split<FFT, G::WS>(v, t, buf, [&](int m, float2 A, float2 B) {
+                const int k = t + m * T;
+                acc[k] += A.x * A.x + A.y * A.y;
+                acc[FFT + k] += B.x * B.x + B.y * B.y;
                 acc[2 * FFT + k] += A.x * B.x + A.y * B.y;
                 acc[3 * FFT + k] += A.y * B.x - A.x * B.y;
-            } else {
-                acc[k] += pa + pb;  // B is zero when frame 2i+1 does not exist
-            }
-        });
+            });
+        } else {
+            // |A_k|^2 + |B_k|^2 = (|Z_k|^2 + |Z_{n-k}|^2) / 2 for A, B the spectra
+            // of the real and imaginary inputs: sum |Z_k|^2 here, fold k and n-k
+            // once per walker below (no Hermitian split per line; a missing
+            // frame 2i+1 leaves Z Hermitian and the fold gives |A_k|^2)
+#pragma unroll
+            for (int m = 0; m < SP_E; ++m) acc[t + m * T] += v[m].x * v[m].x + v[m].y * v[m].y;
+        }
+    }
+    if constexpr (!COH) {
+        __syncthreads();  // every thread's sums are written
+        float fold[SP_E];
+#pragma unroll
+        for (int m = 0; m < SP_E; ++m) {
+            const int k = t + m * T;
+            fold[m] = 0.5f * (acc[k] + acc[(FFT - k) & (FFT - 1)]);
+        }
+        __syncthreads();  // every read of the unfolded sums is done
+#pragma unroll
+        for (int m = 0; m < SP_E; ++m) acc[t + m * T] = fold[m];
+        if constexpr (ACC_SMEM) __syncthreads();
     }
     if constexpr (ACC_SMEM) {
         float* dst = part + u * PLANES * FFT;

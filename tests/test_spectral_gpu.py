@@ -49,7 +49,9 @@ def test_stft_odd_and_zero_frame_counts(M):
 
 @pytest.mark.parametrize("fft,hop,kind,n", [
     (64, 32, 0, 10000), (256, 128, 1, 1 << 18), (4096, 2048, 0, 1 << 20), (8192, 2048, 4, 1 << 20),
-    (16384, 8192, 0, 1 << 20)])
+    (16384, 8192, 0, 1 << 20),
+    (1024, 512, 0, 1024),                # one frame: its line's imaginary input is zero
+    (2048, 1000, 3, 2048 + 2 * 1000)])   # three frames: the last pair holds one
 def test_welch_matches_fp64(M, fft, hop, kind, n):
     x = np.random.default_rng(n + fft).standard_normal(n).astype(np.float32)
     wt = M.WindowType(kind, 6.0)
