@@ -181,12 +181,17 @@ __global__ void __launch_bounds__(SpGeom<FFT>::THREADS, SpGeom<FFT>::MINB)
         }
         fft_regs<FFT, SP_E, G::WS>(v, t, buf, tw);
         if constexpr (COH) {
+            // bins 0 .. n/2 only: for real frames A_{n-k} and B_{n-k} are the
+            // exact conjugates of A_k and B_k, so the sums at n - k mirror
+            // these (k_spec_finish reads them there)
             hermitian_split<FFT, G::WS>(v, t, buf, [&](int m, float2 A, float2 B) {
                 const int k = t + m * T;
-                acc[k] += A.x * A.x + A.y * A.y;
-                acc[FFT + k] += B.x * B.x + B.y * B.y;
-                acc[2 * FFT + k] += A.x * B.x + A.y * B.y;
-                acc[3 * FFT + k] += A.y * B.x - A.x * B.y;
+                if (k <= FFT / 2) {
+                    acc[k] += A.x * A.x + A.y * A.y;
+                    acc[FFT + k] += B.x * B.x + B.y * B.y;
+                    acc[2 * FFT + k] += A.x * B.x + A.y * B.y;
+                    acc[3 * FFT + k] += A.y * B.x - A.x * B.y;
+                }
             });
         } else {
             // |A_k|^2 + |B_k|^2 = (|Z_k|^2 + |Z_{n-k}|^2) / 2 for A, B the spectra
@@ -226,12 +231,15 @@ __global__ void k_spec_finish(const float* __restrict__ part, long long units, i
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= fft) return;
     constexpr int PLANES = COH ? 4 : 1;
+    // coherence sums exist for bins 0 .. n/2; bin k > n/2 has those of n - k
+    // (|Sxy|^2, Sxx and Syy are symmetric)
+    const int ks = (COH && k > fft / 2) ? fft - k : k;
     double s[PLANES];
 #pragma unroll
     for (int pl = 0; pl < PLANES; ++pl) s[pl] = 0.0;
     for (long long u = 0; u < units; ++u)
 #pragma unroll
-        for (int pl = 0; pl < PLANES; ++pl) s[pl] += part[(u * PLANES + pl) * fft + k];
+        for (int pl = 0; pl < PLANES; ++pl) s[pl] += part[(u * PLANES + pl) * fft + ks];
     if constexpr (COH) {
         const double den = s[0] * s[1];
         out[k] = den > 0.0 ? (float)((s[2] * s[2] + s[3] * s[3]) / den) : 0.f;
