@@ -309,18 +309,44 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
 }
 
 // dphi[p] = sum over tiles (fixed order); loss = sum of the tile losses
-__global__ void k_sar_reduce(const float* __restrict__ part, long long tiles, long long na, float* __restrict__ dphi,
-                             const double* __restrict__ loss_part, double* __restrict__ loss) {
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < na) {
+// dphi[p] = sum over tiles of part[tile][p], loss = sum of loss_part: FP64 in a
+// fixed order.  CTA b < ceil(na / 32) owns pulses 32b .. 32b + 31 (lane = pulse,
+// so a warp reads 128 contiguous bytes of a tile); its 32 warps sum contiguous
+// runs of tiles in tile order, then lane l adds the 32 runs in warp order.  The
+// last CTA sums the loss partials: contiguous runs per thread, then a fixed
+// pairwise tree.
+constexpr int SAR_RED_THREADS = 1024;
+__global__ void __launch_bounds__(SAR_RED_THREADS)
+    k_sar_reduce(const float* __restrict__ part, long long tiles, long long na, float* __restrict__ dphi,
+                 const double* __restrict__ loss_part, double* __restrict__ loss) {
+    __shared__ double red[SAR_RED_THREADS];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const long long pulse_ctas = (na + 31) / 32;
+    if (blockIdx.x < pulse_ctas) {
+        const long long p = (long long)blockIdx.x * 32 + l;
+        const long long run = (tiles + 31) / 32, i0 = w * run, i1 = i0 + run < tiles ? i0 + run : tiles;
         double s = 0.0;
-        for (long long i = 0; i < tiles; ++i) s += part[i * na + p];
-        dphi[p] = (float)s;
-    }
-    if (p == 0 && loss) {
+        if (p < na)
+            for (long long i = i0; i < i1; ++i) s += part[i * na + p];
+        red[threadIdx.x] = s;
+        __syncthreads();
+        if (w == 0 && p < na) {
+            double t = 0.0;
+            for (int q = 0; q < 32; ++q) t += red[q * 32 + l];
+            dphi[p] = (float)t;
+        }
+    } else if (loss) {
+        const long long run = (tiles + SAR_RED_THREADS - 1) / SAR_RED_THREADS, i0 = threadIdx.x * run;
+        const long long i1 = i0 + run < tiles ? i0 + run : tiles;
         double s = 0.0;
-        for (long long i = 0; i < tiles; ++i) s += loss_part[i];
-        *loss = s;
+        for (long long i = i0; i < i1; ++i) s += loss_part[i];
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int h = SAR_RED_THREADS / 2; h > 0; h >>= 1) {
+            if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) *loss = red[0];
     }
 }
 
@@ -716,8 +742,8 @@ extern "C" int mfft_sar_backward_phase(mfft_sar* s, const void* raw_h, const flo
     sar_pass_a(s, raw_h, pulse_scale, phase, st);
     s->ak->bwd((int)s->tiles, st, s->rc, s->rc_scale, s->prm.range_n, s->tw_a, nullptr, nullptr, s->dphi_part,
                s->loss_part);
-    k_sar_reduce<<<(unsigned)((s->prm.pulses + 255) / 256), 256, 0, st>>>(s->dphi_part, s->tiles, s->prm.pulses, dphi,
-                                                                          s->loss_part, loss);
+    k_sar_reduce<<<(unsigned)((s->prm.pulses + 31) / 32 + 1), SAR_RED_THREADS, 0, st>>>(
+        s->dphi_part, s->tiles, s->prm.pulses, dphi, s->loss_part, loss);
     return sar_check_launch("SAR backward");
 }
 
@@ -726,8 +752,8 @@ static void sar_enqueue_step(mfft_sar* s, const void* raw_h, const float* ps, co
     sar_pass_a(s, raw_h, ps, ph, st);
     s->ak->both((int)s->tiles, st, s->rc, s->rc_scale, s->prm.range_n, s->tw_a, (__half2*)image_h, image_scale,
                 s->dphi_part, s->loss_part);
-    k_sar_reduce<<<(unsigned)((s->prm.pulses + 255) / 256), 256, 0, st>>>(s->dphi_part, s->tiles, s->prm.pulses, dphi,
-                                                                          s->loss_part, loss);
+    k_sar_reduce<<<(unsigned)((s->prm.pulses + 31) / 32 + 1), SAR_RED_THREADS, 0, st>>>(
+        s->dphi_part, s->tiles, s->prm.pulses, dphi, s->loss_part, loss);
 }
 
 extern "C" int mfft_sar_step_graph(mfft_sar* s, const void* raw_h, const float* pulse_scale, const float* phase,
