@@ -258,13 +258,25 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
     }
 }
 
-// sum of the walkers' dh spectra, one thread per bin, fixed order
-__global__ void k_sum_spectra(const float2* __restrict__ part, long long units, int fft, float2* __restrict__ out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= fft) return;
+// sum of the walkers' dh spectra in a fixed order: a CTA owns 16 consecutive
+// bins; thread (run r, bin b) sums walkers [r*R, (r+1)*R) of its bin in walker
+// order, then lane b adds the 16 runs in run order (fft/16 CTAs)
+constexpr int SUM_BINS = 16, SUM_RUNS = 16;
+__global__ void __launch_bounds__(SUM_BINS * SUM_RUNS)
+    k_sum_spectra(const float2* __restrict__ part, long long units, int fft, float2* __restrict__ out) {
+    __shared__ float2 red[SUM_RUNS][SUM_BINS];
+    const int b = threadIdx.x % SUM_BINS, r = threadIdx.x / SUM_BINS;
+    const int k = blockIdx.x * SUM_BINS + b;  // fft is a multiple of SUM_BINS
+    const long long run = (units + SUM_RUNS - 1) / SUM_RUNS, u0 = r * run;
+    const long long u1 = u0 + run < units ? u0 + run : units;
     float2 s = make_float2(0.f, 0.f);
-    for (long long u = 0; u < units; ++u) s = cadd(s, part[u * fft + k]);
-    out[k] = s;
+    for (long long u = u0; u < u1; ++u) s = cadd(s, part[u * fft + k]);
+    red[r][b] = s;
+    __syncthreads();
+    if (r != 0) return;
+    float2 tot = make_float2(0.f, 0.f);
+    for (int q = 0; q < SUM_RUNS; ++q) tot = cadd(tot, red[q][b]);
+    out[k] = tot;
 }
 
 // dh[k] = Re IFFT(D)[k], k < K (one line)
@@ -608,7 +620,8 @@ static int conv_bwd_device(mfft_conv* c, const float* x, long long nx, const flo
     c->lk->bwd(dim3((unsigned)ctas), c->lk->smem, s, x, nx, gy, ny, c->H, c->tw, (int)c->hop, nblocks, bpu,
                dx ? dx : reinterpret_cast<float*>(c->part) /* unused when nblocks==0 */, c->part);
     if (dh) {
-        k_sum_spectra<<<(unsigned)((c->fft + 255) / 256), 256, 0, s>>>(c->part, slots, (int)c->fft, c->Dsum);
+        k_sum_spectra<<<(unsigned)(c->fft / SUM_BINS), SUM_BINS * SUM_RUNS, 0, s>>>(c->part, slots, (int)c->fft,
+                                                                                 c->Dsum);
         c->lk->dh(s, c->Dsum, c->tw, (int)c->K, dh);
     }
     cudaError_t e = cudaGetLastError();

@@ -224,22 +224,39 @@ __global__ void __launch_bounds__(SpGeom<FFT>::THREADS, SpGeom<FFT>::MINB)
     }
 }
 
-// one thread per bin: fixed-order sum over walkers, then the normalisation
+// Sum over walkers, then the normalisation.  A CTA owns 16 consecutive bins;
+// thread (run r, bin b) sums walkers [r*R, (r+1)*R) of its bin in walker order
+// (FP64), and lane b then adds the 16 runs in run order: a fixed order, with
+// fft/16 CTAs instead of one serial thread per bin.
+constexpr int FIN_BINS = 16, FIN_RUNS = 16;
 template <bool COH>
-__global__ void k_spec_finish(const float* __restrict__ part, long long units, int fft, float scale,
-                              float* __restrict__ out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= fft) return;
+__global__ void __launch_bounds__(FIN_BINS * FIN_RUNS)
+    k_spec_finish(const float* __restrict__ part, long long units, int fft, float scale, float* __restrict__ out) {
     constexpr int PLANES = COH ? 4 : 1;
+    __shared__ double red[FIN_RUNS][PLANES][FIN_BINS];
+    const int b = threadIdx.x % FIN_BINS, r = threadIdx.x / FIN_BINS;
+    const int k = blockIdx.x * FIN_BINS + b;  // fft is a multiple of FIN_BINS
     // coherence sums exist for bins 0 .. n/2; bin k > n/2 has those of n - k
     // (|Sxy|^2, Sxx and Syy are symmetric)
     const int ks = (COH && k > fft / 2) ? fft - k : k;
+    const long long run = (units + FIN_RUNS - 1) / FIN_RUNS, u0 = r * run;
+    const long long u1 = u0 + run < units ? u0 + run : units;
     double s[PLANES];
 #pragma unroll
     for (int pl = 0; pl < PLANES; ++pl) s[pl] = 0.0;
-    for (long long u = 0; u < units; ++u)
+    for (long long u = u0; u < u1; ++u)
 #pragma unroll
         for (int pl = 0; pl < PLANES; ++pl) s[pl] += part[(u * PLANES + pl) * fft + ks];
+#pragma unroll
+    for (int pl = 0; pl < PLANES; ++pl) red[r][pl][b] = s[pl];
+    __syncthreads();
+    if (r != 0) return;
+#pragma unroll
+    for (int pl = 0; pl < PLANES; ++pl) {
+        double tot = 0.0;
+        for (int q = 0; q < FIN_RUNS; ++q) tot += red[q][pl][b];
+        s[pl] = tot;
+    }
     if constexpr (COH) {
         const double den = s[0] * s[1];
         out[k] = den > 0.0 ? (float)((s[2] * s[2] + s[3] * s[3]) / den) : 0.f;
@@ -904,8 +921,9 @@ int acc_device(mfft_spectral* s, bool coh, const float* a, const float* b, long 
         s->part_floats = need;
     }
     s->k->acc(coh, dim3((unsigned)ctas), st, a, b, frames, (int)s->hop, s->window, s->tw, work, per, s->part);
-    if (coh) k_spec_finish<true><<<(unsigned)((s->fft + 255) / 256), 256, 0, st>>>(s->part, slots, (int)s->fft, scale, out);
-    else k_spec_finish<false><<<(unsigned)((s->fft + 255) / 256), 256, 0, st>>>(s->part, slots, (int)s->fft, scale, out);
+    const unsigned fin = (unsigned)(s->fft / FIN_BINS);
+    if (coh) k_spec_finish<true><<<fin, FIN_BINS * FIN_RUNS, 0, st>>>(s->part, slots, (int)s->fft, scale, out);
+    else k_spec_finish<false><<<fin, FIN_BINS * FIN_RUNS, 0, st>>>(s->part, slots, (int)s->fft, scale, out);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "spectral launch");
     return MFFT_SUCCESS;
