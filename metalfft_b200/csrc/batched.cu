@@ -10,6 +10,7 @@
 // coalesced, and the inverse's conjugations and 1/N scale
 // (MetalFFT.swift:56-65) are fused into the load and the store.
 #include "kernels.h"
+#include "pdl.cuh"
 #include "stockham.cuh"
 #include "tma.cuh"
 
@@ -24,30 +25,6 @@ __global__ void k_twiddle_rows(float2* tw, int off, int ns, int radix, int rowle
     tw[off + idx] = make_float2((float)c, (float)s);
 }
 
-// Programmatic dependent launch: a kernel launched with
-// cudaLaunchAttributeProgrammaticStreamSerialization is set up while the
-// previous kernel on the stream drains; grid_dep_wait() (before the first
-// global access) returns once that kernel has completed and its memory is
-// visible, and is a no-op for an ordinary launch.  The previous kernel
-// triggers implicitly at its end: an explicit early trigger let the next
-// grid's CTAs take SM slots too soon (N=4096 x 256 forward + inverse: 11 %
-// slower; the implicit trigger: 2 % faster than no PDL).
-__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
-template <class K, class... Args>
-static cudaError_t launch_pdl(K kernel, unsigned blocks, int threads, int smem, cudaStream_t s, Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
-    cfg.blockDim = dim3((unsigned)threads);
-    cfg.dynamicSmemBytes = (size_t)smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, args...);
-}
 
 template <int N, int E, int FPB, bool INV>
 __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)

@@ -42,6 +42,7 @@
 #include <vector>
 
 #include "capi_internal.h"
+#include "pdl.cuh"
 #include "stockham.cuh"
 
 namespace mfft {
@@ -279,6 +280,9 @@ __global__ void __launch_bounds__(SpGeom<FFT>::THREADS)
     using G = SpGeom<FFT>;
     constexpr int T = G::T, HS = xs_stride(FFT);
     extern __shared__ __align__(16) float2 smem[];
+    // launched as a dependent of the previous chunk's pair kernel, which still
+    // reads X: wait for it before any global access
+    grid_dep_wait();
     const int lf = threadIdx.x / T, t = threadIdx.x % T;
     const PadLine buf{smem + lf * spad_size(FFT)};
     const long long pairs = (nf + 1) / 2;
@@ -418,6 +422,7 @@ __global__ void __launch_bounds__(XS_THREADS, 2)
     k_xspec_acc(const float2* __restrict__ X, int C, int nbins, long long nf, int per, int first,
                 float* __restrict__ part) {
     // CC > 0: the channel count is the compile-time CC (== C)
+    grid_dep_wait();  // the chunk's spectra come from the k_xstft launched just before
     constexpr int KB = XS_THREADS / G, PMAX = xs_pmax(G);
     extern __shared__ __align__(16) float2 stage[];  // [XS_ST][XF][C][KB]
     // byte offsets (channel i, channel j) of every pair inside a frame's
@@ -652,7 +657,8 @@ cudaError_t sp_prepare() {
 template <int FFT>
 void sp_xstft(dim3 grid, cudaStream_t s, const float* x, long long len, int C, long long f0, long long nf, int hop,
               const float* w, const float2* tw, float2* X, float* nyq) {
-    k_xstft<FFT><<<grid, SpGeom<FFT>::THREADS, SpGeom<FFT>::XCH * 8, s>>>(x, len, C, f0, nf, hop, w, tw, X, nyq);
+    launch_pdl(k_xstft<FFT>, grid, SpGeom<FFT>::THREADS, SpGeom<FFT>::XCH * 8, s, x, len, C, f0, nf, hop, w, tw, X,
+               nyq);
 }
 template <int FFT>
 void sp_stft(dim3 grid, cudaStream_t s, const float* x, long long frames, int hop, const float* w, const float2* tw,
@@ -698,7 +704,7 @@ const SpKernels* find_spk(int fft) {
 template <int G, bool COH, int CC = 0>
 void xs_launch(dim3 grid, int smem, cudaStream_t s, const float2* X, int C, int nbins, long long nf, int per,
                int first, float* part) {
-    k_xspec_acc<G, COH, CC><<<grid, XS_THREADS, smem, s>>>(X, C, nbins, nf, per, first, part);
+    launch_pdl(k_xspec_acc<G, COH, CC>, grid, XS_THREADS, smem, s, X, C, nbins, nf, per, first, part);
 }
 using XsFn = void (*)(dim3, int, cudaStream_t, const float2*, int, int, long long, int, int, float*);
 // channel counts 2, 4 and 8 have a compile-time kernel (G = xs_groups(C))
