@@ -751,8 +751,9 @@ int xs_occ(int g, bool coh, int smem, int C) {
 }
 
 // spectra of one chunk stay at most this large (L2 holds them until the
-// accumulation reads them back)
-constexpr long long XS_CHUNK_BYTES = 32ll << 20;
+// accumulation reads them back; 8 channels at fftSize 1024: 48 MiB chunks
+// 0.636 ms per call, 32 MiB 0.675 ms, 64 MiB 0.649 ms)
+constexpr long long XS_CHUNK_BYTES = 48ll << 20;
 
 }  // namespace
 
