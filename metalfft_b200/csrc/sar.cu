@@ -116,19 +116,26 @@ __global__ void k_sar_power(const float2* __restrict__ raw, long long n, double*
     }
 }
 
-// complex Gaussian noise: per-sample Box-Muller on two counter-based uniforms,
-// std per component sqrt(P / (2 * 10^(snr/10))), P from the partial sums
-__global__ void k_sar_noise(float2* __restrict__ raw, long long n, const double* __restrict__ part, int nparts,
-                            double snr_db, uint64_t seed) {
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
+// the noise standard deviation per component, once: the partial sums added in
+// block order (FP64), sqrt(P / (2 * 10^(snr/10))) with P the mean |s|^2 of the
+// non-zero samples; -1 when every sample is zero (no noise is added)
+__global__ void k_sar_sigma(double* __restrict__ part, int nparts, double snr_db) {
+    if (threadIdx.x != 0) return;
     double s = 0.0, c = 0.0;
     for (int i = 0; i < nparts; ++i) {
         s += part[2 * i];
         c += part[2 * i + 1];
     }
-    if (c <= 0.0) return;
-    const double sigma = sqrt((s / c) / pow(10.0, snr_db / 10.0) / 2.0);
+    part[2 * nparts] = c <= 0.0 ? -1.0 : sqrt((s / c) / pow(10.0, snr_db / 10.0) / 2.0);
+}
+
+// complex Gaussian noise: per-sample Box-Muller on two counter-based uniforms,
+// std per component *sigma_p (k_sar_sigma)
+__global__ void k_sar_noise(float2* __restrict__ raw, long long n, const double* __restrict__ sigma_p, uint64_t seed) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const double sigma = *sigma_p;
+    if (sigma < 0.0) return;
     const double u1 = unit_open(seed, 2 * (uint64_t)idx), u2 = unit_open(seed, 2 * (uint64_t)idx + 1);
     const double rr = sigma * sqrt(-2.0 * log(u1));
     double sn, cs;
@@ -602,13 +609,14 @@ extern "C" int mfft_sar_simulate(mfft_ctx* ctx, const mfft_sar_params* p, const 
     double* part = nullptr;
     const int nparts = 1024;
     cudaError_t e = cudaMallocAsync(&dt, sizeof(mfft_sar_target) * (ntargets > 0 ? ntargets : 1), s);
-    if (e == cudaSuccess) e = cudaMallocAsync(&part, sizeof(double) * 2 * nparts, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&part, sizeof(double) * (2 * nparts + 1), s);
     if (e != cudaSuccess) return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "simulator buffers: %s", cudaGetErrorString(e));
     if (ntargets > 0) e = cudaMemcpyAsync(dt, targets, sizeof(mfft_sar_target) * ntargets, cudaMemcpyHostToDevice, s);
     const unsigned blocks = (unsigned)((n + 255) / 256);
     k_sar_signal<<<blocks, 256, 0, s>>>((float2*)raw, g, dt, ntargets);
     k_sar_power<<<nparts, 256, 0, s>>>((const float2*)raw, n, part);
-    k_sar_noise<<<blocks, 256, 0, s>>>((float2*)raw, n, part, nparts, snr_db, seed);
+    k_sar_sigma<<<1, 32, 0, s>>>(part, nparts, snr_db);
+    k_sar_noise<<<blocks, 256, 0, s>>>((float2*)raw, n, part + 2 * nparts, seed);
     cudaFreeAsync(dt, s);
     cudaFreeAsync(part, s);
     e = cudaGetLastError();
