@@ -66,26 +66,45 @@ __device__ inline double unit_open(uint64_t seed, uint64_t idx) {
     return ((double)(mix64(seed ^ mix64(idx)) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
 }
 
-__global__ void k_sar_signal(float2* __restrict__ raw, SarGeom g, const mfft_sar_target* __restrict__ tg, int nt) {
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= g.na * g.nr) return;
-    const long long p = idx / g.nr, r = idx % g.nr;
+// A CTA covers SIG_T consecutive range samples of one pulse (blockIdx.x =
+// pulse * chunks + chunk).  The slant range R of each target depends on the
+// pulse only: the CTA forms R, 2R/c and 4 pi R / lambda once per target (in
+// shared memory, SIG_T targets at a time) and every sample reads them, with
+// the same FP64 expressions as a per-sample evaluation.
+constexpr int SIG_T = 256;
+__global__ void __launch_bounds__(SIG_T)
+    k_sar_signal(float2* __restrict__ raw, SarGeom g, const mfft_sar_target* __restrict__ tg, int nt) {
+    __shared__ double s_delay[SIG_T], s_rph[SIG_T], s_ph[SIG_T], s_amp[SIG_T];
+    const long long chunks = (g.nr + SIG_T - 1) / SIG_T;
+    const long long p = blockIdx.x / chunks, r = (blockIdx.x % chunks) * SIG_T + threadIdx.x;
     const double eta = (double)(p - g.na / 2) / g.prf;
     const double tr = g.tau0 + (double)r / g.fs;
     double re = 0.0, im = 0.0;
-    for (int i = 0; i < nt; ++i) {
-        const double dx = g.v * eta - tg[i].azimuth_m;
-        const double R = sqrt(tg[i].range_m * tg[i].range_m + dx * dx);
-        const double dt = tr - 2.0 * R / C_LIGHT;
-        if (fabs(dt) <= g.tp / 2.0) {
-            const double ph = PI_D * g.kr * dt * dt - 4.0 * PI_D * R / g.lambda + tg[i].phase;
-            double s, c;
-            sincos(ph, &s, &c);
-            re += tg[i].amplitude * c;
-            im += tg[i].amplitude * s;
+    for (int i0 = 0; i0 < nt; i0 += SIG_T) {
+        const int i = i0 + threadIdx.x;
+        if (i < nt) {
+            const double dx = g.v * eta - tg[i].azimuth_m;
+            const double R = sqrt(tg[i].range_m * tg[i].range_m + dx * dx);
+            s_delay[threadIdx.x] = 2.0 * R / C_LIGHT;
+            s_rph[threadIdx.x] = 4.0 * PI_D * R / g.lambda;
+            s_ph[threadIdx.x] = tg[i].phase;
+            s_amp[threadIdx.x] = tg[i].amplitude;
         }
+        __syncthreads();
+        const int n = nt - i0 < SIG_T ? nt - i0 : SIG_T;
+        for (int j = 0; j < n; ++j) {
+            const double dt = tr - s_delay[j];
+            if (fabs(dt) <= g.tp / 2.0) {
+                const double ph = PI_D * g.kr * dt * dt - s_rph[j] + s_ph[j];
+                double sn, cs;
+                sincos(ph, &sn, &cs);
+                re += s_amp[j] * cs;
+                im += s_amp[j] * sn;
+            }
+        }
+        __syncthreads();
     }
-    raw[idx] = make_float2((float)re, (float)im);
+    if (r < g.nr) raw[p * g.nr + r] = make_float2((float)re, (float)im);
 }
 
 // per-block partial sums of |s|^2 over non-zero samples and their count
@@ -613,7 +632,7 @@ extern "C" int mfft_sar_simulate(mfft_ctx* ctx, const mfft_sar_params* p, const 
     if (e != cudaSuccess) return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "simulator buffers: %s", cudaGetErrorString(e));
     if (ntargets > 0) e = cudaMemcpyAsync(dt, targets, sizeof(mfft_sar_target) * ntargets, cudaMemcpyHostToDevice, s);
     const unsigned blocks = (unsigned)((n + 255) / 256);
-    k_sar_signal<<<blocks, 256, 0, s>>>((float2*)raw, g, dt, ntargets);
+    k_sar_signal<<<(unsigned)(g.na * ((g.nr + SIG_T - 1) / SIG_T)), SIG_T, 0, s>>>((float2*)raw, g, dt, ntargets);
     k_sar_power<<<nparts, 256, 0, s>>>((const float2*)raw, n, part);
     k_sar_sigma<<<1, 32, 0, s>>>(part, nparts, snr_db);
     k_sar_noise<<<blocks, 256, 0, s>>>((float2*)raw, n, part + 2 * nparts, seed);
