@@ -118,7 +118,8 @@ __device__ __forceinline__ float line_scale(float mx) {
 // lines in flight per SM where two CTAs of one pipeline each hold two (and
 // two copies of the operand).  A pipeline's four warps cover the 128 TMEM
 // lanes, each walking both 32-column halves of D1 and D2; lines are loaded
-// directly (no register prefetch: the other pipelines cover the latency).
+// directly into registers, the pipeline's next line prefetched into L2 one
+// line ahead (split 33.1 -> 34.6 M, BF16 45.9 -> 48.9 M transforms/s).
 constexpr int TQ_PIPES = 4, TQ_PT = 128, TQ_THREADS = TQ_PIPES * TQ_PT;
 constexpr uint32_t TQ_B = 65536, TQ_BSTRIDE = 32768;          // pipeline p: B hi at TQ_B + p*TQ_BSTRIDE, lo +16 KB
 constexpr uint32_t TQ_T1 = TQ_B + TQ_PIPES * TQ_BSTRIDE;      // W4096^(i*k1), i < 16: 8 KB
@@ -162,6 +163,11 @@ __device__ __forceinline__ void issue_product_q(uint32_t d_tmem, uint32_t g_addr
             tc::mma_f16_ss(d_tmem, ad, bd, idesc, (pr > 0 || j > 0) ? 1u : 0u);
         }
     }
+}
+
+// bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned) into L2
+__device__ __forceinline__ void prefetch_l2(const void* g, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ void pipe_sync(int p) {
@@ -217,7 +223,10 @@ __global__ void __launch_bounds__(TQ_THREADS, 1)
 
     uint32_t phase = 0;
     bool aborted = false;
-    for (long long f = (long long)blockIdx.x * TQ_PIPES + p; f < batch; f += (long long)gridDim.x * TQ_PIPES) {
+    const long long fstep = (long long)gridDim.x * TQ_PIPES;
+    for (long long f = (long long)blockIdx.x * TQ_PIPES + p; f < batch; f += fstep) {
+        // this pipeline's next line to L2 while this one goes through both stages
+        if (ptid == 0 && f + fstep < batch) prefetch_l2(in + (size_t)(f + fstep) * TC_N, TC_N * sizeof(float2));
         // ---- the line, its scale, the stage-1 operand (MN-major) ----
         float4 cur[16];
         const float4* src = reinterpret_cast<const float4*>(in + (size_t)f * TC_N);
