@@ -28,7 +28,8 @@ def _rel(a, b):
 @pytest.mark.parametrize("C,fft,hop,kind,n", [
     (1, 256, 128, 0, 4096), (2, 64, 32, 1, 5000), (3, 1024, 512, 0, 1 << 14), (6, 512, 200, 4, 30000),
     (7, 1024, 512, 0, 1 << 15), (8, 4096, 1024, 2, 1 << 16), (9, 256, 128, 0, 20000), (12, 2048, 1024, 0, 1 << 15),
-    (16, 1024, 512, 0, 512 * 1201 + 512), (16, 16384, 8192, 0, 8192 * 33), (5, 64, 64, 0, 64 * 2100 + 7)])
+    (16, 1024, 512, 0, 512 * 1201 + 512), (16, 16384, 8192, 0, 8192 * 33), (5, 64, 64, 0, 64 * 2100 + 7),
+    (4, 512, 256, 1, 1 << 14)])
 def test_cross_spectral_matches_fp64(M, C, fft, hop, kind, n):
     rng = np.random.default_rng(C * 1000 + fft)
     base = rng.standard_normal(n)
@@ -130,3 +131,21 @@ def test_device_tensors_match_host(M):
     # repeated calls on one handle are deterministic (fixed-order sums)
     dp2, dc2, dh2 = est.cross_spectral(torch.from_numpy(x).cuda())
     assert torch.equal(dp, dp2) and torch.equal(dc, dc2) and torch.equal(dh, dh2)
+
+
+@pytest.mark.parametrize("C,fft", [(2, 256), (4, 1024), (8, 1024)])
+def test_welch_mode_compile_time_channel_counts(M, C, fft):
+    # 2, 4 and 8 channels take the kernel whose channel count is a template
+    # constant; the Welch estimate |mean S_ij|^2 / (mean p_i mean p_j) against
+    # the FP64 oracle's averaged powers and cross-spectra
+    rng = np.random.default_rng(C + fft)
+    n = fft * 40 + 3
+    base = rng.standard_normal(n)
+    x = np.stack([0.5 * base + rng.standard_normal(n) for _ in range(C)]).astype(np.float32)
+    rw = M.PSD.cross_spectral(x, fft, fft // 2, 48000.0, coherence_mode=M.COHERENCE_WELCH)
+    pw, cr, _ = O.cross_spectral64(x.astype(np.float64), fft, fft // 2, _w(0, fft))
+    assert float(np.max(np.abs(rw.power - pw)) / pw.max()) < 3e-6
+    assert _rel(rw.cross_spectra, cr) < 1e-5
+    ii, jj = np.triu_indices(C, 1)
+    den = pw[ii] * pw[jj]
+    assert float(np.max(np.abs(rw.coherence - np.abs(cr) ** 2 / den))) < 1e-5
