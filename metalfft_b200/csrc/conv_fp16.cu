@@ -170,6 +170,11 @@ __device__ __forceinline__ void hpass(typename A::V (&v)[FH_E], int t, __half2* 
     }
 }
 
+// number of valid samples in a window of `cap` when `avail` remain (0 .. cap)
+__device__ __forceinline__ int fh_count(long long avail, int cap) {
+    return avail <= 0 ? 0 : (avail >= cap ? cap : (int)avail);
+}
+
 template <int MODE>
 struct FhPolicy;
 template <>
@@ -220,16 +225,18 @@ __global__ void __launch_bounds__(FH_T, 2)
     for (long long it = 0; it < iters; ++it) {
         const long long p = pw + it;
         const long long b = 2 * p;
+        // 32-bit offsets from the pair's first sample: lim0 / lim1 = valid
+        // samples of blocks b and b+1
+        const long long base = b * hop;
+        const float* xb = x + base;
+        const int lim0 = fh_count(nx - base, hop), lim1 = fh_count(nx - base - hop, hop);
         V v[FH_E];
 #pragma unroll
         for (int m = 0; m < FH_E; ++m) {
             const int i = t + m * FH_T;
-            const long long s0 = b * hop + i, s1 = s0 + hop;
             float re = 0.f, im = 0.f;
-            if (i < hop) {
-                if (s0 < nx) re = __ldcs(x + s0);
-                if (s1 < nx) im = __ldcs(x + s1);
-            }
+            if (i < lim0) re = __ldcs(xb + i);
+            if (i < lim1) im = __ldcs(xb + hop + i);
             if constexpr (MODE == MFFT_CONV_FP16_PURE) v[m] = __floats2half2_rn(re, im);
             else v[m] = make_float2(re, im);
         }
@@ -256,13 +263,15 @@ __global__ void __launch_bounds__(FH_T, 2)
             else return make_float2(v[m].x * sc, -v[m].y * sc);
         };
         const bool write = p >= p0;
+        float* yb = y + base;
+        const int wlim0 = write ? fh_count(ny - base, hop) : 0;
+        const int wlim1 = write ? fh_count(ny - base - hop, hop) : 0;
 #pragma unroll
         for (int m = 0; m < FH_E; ++m) {
             const int i = t + m * FH_T;
             const float val = out(m).x + acc0[i];
             if (i < hop) {
-                const long long o = b * hop + i;
-                if (write && o < ny) __stcs(y + o, val);
+                if (i < wlim0) __stcs(yb + i, val);
             } else {
                 acc1[i - hop] = val;
             }
@@ -273,8 +282,7 @@ __global__ void __launch_bounds__(FH_T, 2)
             const int i = t + m * FH_T;
             const float val = out(m).y + acc1[i];
             if (i < hop) {
-                const long long o = (b + 1) * hop + i;
-                if (write && o < ny) __stcs(y + o, val);
+                if (i < wlim1) __stcs(yb + hop + i, val);
             } else {
                 acc0[i - hop] = val;
             }
