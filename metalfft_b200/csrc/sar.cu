@@ -259,11 +259,14 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
     const long long tile = blockIdx.x;
     const int c = threadIdx.x % C, t = threadIdx.x / C;
     const long long col = tile * C + c;
+    // rows t + m*T of column col: a base pointer and a stride of T rows
+    const __half2* rcol = rc + (long long)t * nr + col;
+    const long long rstep = (long long)T * nr;
     float2 v[SAR_E];
 #pragma unroll
     for (int m = 0; m < SAR_E; ++m) {
         const int p = t + m * T;
-        const float2 u = __half22float2(rc[(long long)p * nr + col]);
+        const float2 u = __half22float2(rcol[m * rstep]);
         const float s = __ldg(rc_scale + p);
         v[m] = make_float2(u.x * s, INV ? -u.y * s : u.y * s);
     }
@@ -289,9 +292,9 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
         for (int i = 0; i < (AzGeom<NA>::THREADS + 31) / 32; ++i) cm = fmaxf(cm, red[i][c]);
         const float s = block_scale(cm);
         const float inv = 1.f / s;
+        __half2* icol = image + (long long)t * nr + col;
 #pragma unroll
-        for (int m = 0; m < SAR_E; ++m)
-            image[(long long)(t + m * T) * nr + col] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
+        for (int m = 0; m < SAR_E; ++m) icol[m * rstep] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
         if (t == 0) image_scale[col] = s;
     }
     if constexpr (GRAD) {
@@ -307,7 +310,7 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
 #pragma unroll
         for (int m = 0; m < SAR_E; ++m) {
             const int p = t + m * T;
-            const float2 u0 = __half22float2(rc[(long long)p * nr + col]);
+            const float2 u0 = __half22float2(rcol[m * rstep]);
             const float s = __ldg(rc_scale + p);
             const float2 u = make_float2(u0.x * s, u0.y * s);
             // -Im(u conj(B)) with v = conj(B): -Im(u v)
