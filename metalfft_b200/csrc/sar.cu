@@ -217,9 +217,10 @@ __global__ void __launch_bounds__(NR / SAR_E) k_sar_range(const __half2* __restr
     sincosf(phase[p], &sp, &cp);
     const float sc = pscale[p];
     const float2 rot = make_float2(cp * sc, sp * sc);
+    const __half2* rawp = raw + p * NR + t;  // this thread's samples t + m*T of pulse p
     float2 v[SAR_E];
 #pragma unroll
-    for (int m = 0; m < SAR_E; ++m) v[m] = cmul(__half22float2(raw[p * NR + t + m * T]), rot);
+    for (int m = 0; m < SAR_E; ++m) v[m] = cmul(__half22float2(rawp[m * T]), rot);
     fft_regs<NR, SAR_E, (T <= 32)>(v, t, PadLine{smem}, tw);
 #pragma unroll
     for (int m = 0; m < SAR_E; ++m) v[m] = cconj(cmul(v[m], __ldg(H + t + m * T)));
@@ -233,8 +234,9 @@ __global__ void __launch_bounds__(NR / SAR_E) k_sar_range(const __half2* __restr
     }
     const float s = block_scale(cta_max(mx, red));
     const float inv = 1.f / s;
+    __half2* rcp = rc + p * NR + t;
 #pragma unroll
-    for (int m = 0; m < SAR_E; ++m) rc[p * NR + t + m * T] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
+    for (int m = 0; m < SAR_E; ++m) rcp[m * T] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
     if (t == 0) rc_scale[p] = s;
 }
 
