@@ -4,8 +4,7 @@
  *
  * The reference's public boundary is a Swift API (docs/MetalFFT.swiftinterface
  * :12-266).  Every entry point below names the Swift declaration it replaces;
- * a Swift/C++/Python wrapper re-creates that API on top (the Swift module map
- * and wrapper are given in INTEGRATION.md, the Python mirror is
+ * a Swift/C++/Python wrapper re-creates that API on top (the Python mirror is
  * metalfft_b200/__init__.py, the C++ mirror is metalfft_b200/MetalFFT.hpp).
  *
  * Conventions
@@ -187,6 +186,21 @@ MFFT_API int mfft_plan_kernel_info(const mfft_plan* plan, int* radix, int* lines
 MFFT_API int mfft_exec_c2c(mfft_plan* plan, const void* in, void* out, int64_t batch, int direction,
                   int flags, void* stream);
 
+/* Adjoint (backward) of mfft_exec_c2c, for gradients through the FFT (no
+ * reference counterpart: the reference has no backward pass; its transform
+ * conventions are MetalFFT.swift:56-65 and fft_multisize.metal:70).  For a
+ * real loss L of the transform's output y with grad_out = dL/dRe(y) +
+ * i dL/dIm(y), writes grad_in = dL/dRe(x) + i dL/dIm(x) for the call's input
+ * x, i.e. the conjugate transpose of the transform applied to grad_out:
+ *   direction MFFT_FORWARD (y = F x, unscaled):   grad_in = F^H grad_out
+ *                                                 = n * inverse(grad_out)
+ *   direction MFFT_INVERSE (y = F^H x / n):       grad_in = F grad_out / n
+ * Same kernels as mfft_exec_c2c with the direction swapped and the 1/n scale
+ * moved to the other side in their stores; same sizes, layout, flags and
+ * in-place rule. */
+MFFT_API int mfft_exec_c2c_backward(mfft_plan* plan, const void* grad_out, void* grad_in, int64_t batch,
+                                    int direction, int flags, void* stream);
+
 /* Tensor-core DFT-as-matmul path (tcgen05 + TMEM) for n = 4096: the B200 form
  * of src/fft_4096_ct_mma.metal:88-206 (simdgroup_float8x8 CT-DIF).  variant:
  * MFFT_TC_FP16_SPLIT3 or MFFT_TC_BF16.  Same layout and scaling as
@@ -224,7 +238,8 @@ MFFT_API int mfft_fourstep_noalloc(const void* in, void* out, int64_t n, int64_t
  * in/out buffers.  There is no reference counterpart for a single launch over
  * mixed sizes; it generalises forward(batch:) (MetalFFT.swift:108-133).
  * Sizes up to 4096 run as whole lines, larger ones as four-step transforms
- * whose intermediates stay in a small L2-resident scratch ring. */
+ * (a column pass into an intermediate buffer of the handle holding every
+ * four-step point, then a row pass). */
 typedef struct mfft_multi_desc {
     int64_t n;
     int64_t count;
@@ -401,6 +416,21 @@ MFFT_API int mfft_sar_destroy(mfft_sar* sar);
  * (image[k*range_n + r]) with one scale per range column.  Device memory. */
 MFFT_API int mfft_sar_forward(mfft_sar* sar, const void* raw_h, const float* pulse_scale, const float* phase,
                               void* image_h, float* image_scale, void* stream);
+/* Precision of the range-compressed intermediate between the range pass and
+ * the azimuth pass of later mfft_sar_forward / _backward_phase /
+ * _step_graph calls (no reference counterpart; the reference keeps FP32 device
+ * data and FP16 only in threadgroup memory, fft_sar_fused_fp16.metal:10-33):
+ * MFFT_SAR_RC_FP16 (default): FP16 with one power-of-two scale per pulse,
+ * 4 bytes per sample; MFFT_SAR_RC_FP32: FP32, 8 bytes per sample, allocated
+ * on first selection (pulses x range_n x 8 bytes).  Input and image stay
+ * FP16 in both modes.  The FP32 intermediate is what brings the phase
+ * adjoint to within ~1e-5 of the FP64 gradient of the same FP16 input; the
+ * FP16 one bounds it near 1e-2. */
+enum {
+    MFFT_SAR_RC_FP16 = 0,
+    MFFT_SAR_RC_FP32 = 1
+};
+MFFT_API int mfft_sar_set_intermediate(mfft_sar* sar, int precision);
 /* Adjoint of L = sum |I|^4 with respect to phase (no reference counterpart):
  * dphi[p] = -sum_r Im(u_p[r] conj(B[p][r])), B = sum_k 4|I|^2 I W^{-pk};
  * the loss goes to *loss (device double).  Recomputes the range pass. */

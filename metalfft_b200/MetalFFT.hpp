@@ -4,7 +4,8 @@
 // Reference types (docs/MetalFFT.swiftinterface:12-266) and their mirrors:
 //   FFTError        -> mfft::FFTError (exception; case() names the Swift case)
 //   MetalFFT        -> mfft::MetalFFT: forward, forward(input, output),
-//                      forwardBatch, inverse
+//                      forwardBatch, inverse, backward (adjoint, no
+//                      counterpart)
 //   MultiChannelFFT -> mfft::MultiChannelFFT
 //   Convolver       -> mfft::Convolver: apply, blockSize, hopSize,
 //                      recommendedFFTSize
@@ -86,6 +87,16 @@ class MetalFFT {
         check(mfft_exec_c2c(plan_, input, output.data(), 1, MFFT_FORWARD, MFFT_HOST_MEMORY, nullptr));
     }
     std::vector<cfloat> inverse(const std::vector<cfloat>& x) { return run(x, MFFT_INVERSE); }
+    // Gradient with respect to the input of forward (direction MFFT_FORWARD)
+    // or inverse (MFFT_INVERSE), given the gradient of a real loss with
+    // respect to its output (mfft_exec_c2c_backward).
+    std::vector<cfloat> backward(const std::vector<cfloat>& grad, int direction = MFFT_FORWARD) {
+        if ((int64_t)grad.size() != size_)
+            throw FFTError(MFFT_ERR_INVALID_INPUT_SIZE, "Input size mismatch", size_, (int64_t)grad.size(), -1);
+        std::vector<cfloat> g((size_t)size_);
+        check(mfft_exec_c2c_backward(plan_, grad.data(), g.data(), 1, direction, MFFT_HOST_MEMORY, nullptr));
+        return g;
+    }
     std::vector<std::vector<cfloat>> forwardBatch(const std::vector<std::vector<cfloat>>& xs) {
         if (xs.empty()) return {};
         std::vector<cfloat> flat;

@@ -9,6 +9,7 @@ Reference API (docs/MetalFFT.swiftinterface:12-266) and its mirror here:
     .forward(input:output:)        -> .forward_into(x, out)
     .forward(batch:)               -> .forward_batch(xs)
     .inverse(_:)                   -> .inverse(x)
+    (no counterpart: adjoints)     -> .backward(g, direction) / .backward_batch(gs, direction)
   MultiChannelFFT(channels:size:)  -> MultiChannelFFT(channels, size)
   Convolver(kernel:fftSize:)       -> Convolver(kernel, fft_size)
     .apply(to:) / blockSize / hopSize / recommendedFFTSize(forKernelCount:)
@@ -163,6 +164,42 @@ class MetalFFT:
         _check(st)
         return out
 
+    def exec_backward(self, grad_out, grad_in, batch, direction=FORWARD):
+        """Adjoint of exec on device tensors: grad_in = dL/dx for a real loss
+        L of y = exec(x, direction), given grad_out = dL/dy (complex gradient
+        dL/dRe + i dL/dIm).  FORWARD: n * inverse(grad_out); INVERSE:
+        forward(grad_out) / n."""
+        _check(lib.mfft_exec_c2c_backward(self._plan, ctypes.c_void_p(grad_out.data_ptr()),
+                                          ctypes.c_void_p(grad_in.data_ptr()), batch, direction, DEVICE,
+                                          _stream_of(grad_out)))
+        return grad_in
+
+    def backward(self, grad, direction=FORWARD):
+        """Gradient with respect to the input of forward(_:) (direction
+        FORWARD) or inverse(_:) (INVERSE) of one line."""
+        self._check_len(grad)
+        return self._run_backward(grad, 1, direction)
+
+    def backward_batch(self, grads, direction=FORWARD):
+        """backward of forward(batch:) / the batched inverse: one launch."""
+        a, b = self._batch_array(grads)
+        if b == 0:
+            return np.empty((0, self.size), np.complex64)
+        return self._run_backward(a, b, direction)
+
+    def _run_backward(self, g, batch, direction):
+        if _is_cuda_tensor(g):
+            import torch
+            if g.dtype != torch.complex64:
+                _fail(10, "expected a complex64 tensor, got %s" % g.dtype)
+            g = g.contiguous()
+            return self.exec_backward(g, torch.empty_like(g), batch, direction)
+        a = _host_c64(g)
+        out = np.empty_like(a)
+        _check(lib.mfft_exec_c2c_backward(self._plan, a.ctypes.data, out.ctypes.data, batch, direction, HOST,
+                                          None))
+        return out
+
     def forward_real(self, x):
         """Real input, n/2 + 1 complex bins per line (rfft): host arrays
         ([batch,] n) or a CUDA float32 tensor."""
@@ -309,6 +346,7 @@ class MultiChannelFFT:
 
 from ._dsp import (AnalysisResult, Convolver, Correlator, FFTAnalyzer, FusedConvolver,  # noqa: E402
                    MixedBatch, WindowType)
-from ._sar import SARParameters, SARPipeline, SARTarget, expected_bins, point_target_metrics  # noqa: E402
+from ._sar import (RC_FP16, RC_FP32, SARParameters, SARPipeline, SARTarget, expected_bins,  # noqa: E402
+                   point_target_metrics)
 from ._spectral import (COHERENCE_PER_FRAME, COHERENCE_WELCH, PSD, STFT, CrossSpectralResult,  # noqa: E402
                         SpectralEstimator, STFTFrames, to_decibels)

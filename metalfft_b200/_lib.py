@@ -36,6 +36,7 @@ SIGNATURES = [
     ("mfft_plan_set_kernel", c_int, [c_void_p, c_int, c_int, c_int]),
     ("mfft_list_kernels", c_int, [c_int64, P(c_int), P(c_int), P(c_int), c_int]),
     ("mfft_exec_c2c", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),
+    ("mfft_exec_c2c_backward", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),
     ("mfft_exec_c2c_tc", c_int,
      [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_int, c_void_p]),
     ("mfft_exec_r2c", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p]),
@@ -80,6 +81,7 @@ SIGNATURES = [
     ("mfft_sar_create", c_int, [c_void_p, c_void_p, c_void_p, P(c_void_p)]),
     ("mfft_sar_destroy", c_int, [c_void_p]),
     ("mfft_sar_forward", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("mfft_sar_set_intermediate", c_int, [c_void_p, c_int]),
     ("mfft_sar_backward_phase", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("mfft_sar_step_graph", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_void_p]),

@@ -45,8 +45,13 @@ def _stream(t):
     return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
 
 
+RC_FP16, RC_FP32 = 0, 1
+
+
 class SARPipeline:
-    """Range compression -> corner turn -> azimuth FFT on device tensors."""
+    """Range compression -> corner turn -> azimuth FFT on device tensors.
+    intermediate: RC_FP16 (default, FP16 with per-pulse scales between the
+    passes) or RC_FP32 (the precision the phase adjoint needs for ~1e-5)."""
 
     def __init__(self, params, chirp=None, context=None):
         self.params = params
@@ -55,6 +60,10 @@ class SARPipeline:
         h = ctypes.c_void_p()
         _check(lib.mfft_sar_create(self._ctx, ctypes.byref(params), c.ctypes.data, ctypes.byref(h)))
         self._h = h
+
+    def set_intermediate(self, precision):
+        """RC_FP16 or RC_FP32 for later forward / backward_phase / step calls."""
+        _check(lib.mfft_sar_set_intermediate(self._h, int(precision)))
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -81,11 +81,11 @@ int autotune_batched(mfft_ctx* ctx, int n, long long lines, const BatchedKernel*
         if (ks[i].n != n) continue;
         BatchedBinding bb;
         if (bind_batched(ctx, &ks[i], &bb) != MFFT_SUCCESS) continue;
-        for (int w = 0; w < 3; ++w) ks[i].fwd(a, b, lines, bb.tw, ctx->dev_err, ctx->stream);
+        for (int w = 0; w < 3; ++w) ks[i].fwd(a, b, lines, bb.tw, ctx->dev_err, ctx->stream, 0);
         cudaEventRecord(e0, ctx->stream);
         const int reps = 10;
         for (int r = 0; r < reps; ++r)
-            ks[i].fwd((r & 1) ? b : a, (r & 1) ? a : b, lines, bb.tw, ctx->dev_err, ctx->stream);
+            ks[i].fwd((r & 1) ? b : a, (r & 1) ? a : b, lines, bb.tw, ctx->dev_err, ctx->stream, 0);
         cudaEventRecord(e1, ctx->stream);
         if (cudaEventSynchronize(e1) != cudaSuccess) continue;
         float ms = 0.f;

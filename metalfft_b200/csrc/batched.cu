@@ -26,10 +26,31 @@ __global__ void k_twiddle_rows(float2* tw, int off, int ns, int radix, int rowle
 }
 
 
+// Streams a thread's E results to dst[m*T]: the inverse conjugates and scales
+// by 1/N (MetalFFT.swift:56-65); adj (the adjoint of the transform) drops that
+// scale from the inverse and puts it on the forward.  Power-of-two scalings
+// are exact, so the adjoint of the forward is exactly N x inverse.
+template <int N, int E, bool INV>
+__device__ __forceinline__ void store_line(float2* dst, const float2 (&v)[E], int adj) {
+    constexpr int T = N / E;
+    if constexpr (INV) {
+        const float s = adj ? 1.0f : 1.0f / (float)N;
+#pragma unroll
+        for (int m = 0; m < E; ++m) __stcs(dst + m * T, make_float2(v[m].x * s, -v[m].y * s));
+    } else if (adj) {
+        const float s = 1.0f / (float)N;
+#pragma unroll
+        for (int m = 0; m < E; ++m) __stcs(dst + m * T, make_float2(v[m].x * s, v[m].y * s));
+    } else {
+#pragma unroll
+        for (int m = 0; m < E; ++m) __stcs(dst + m * T, v[m]);
+    }
+}
+
 template <int N, int E, int FPB, bool INV>
 __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
     k_fft_batched(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
-                  const float2* __restrict__ tw) {
+                  const float2* __restrict__ tw, int adj) {
     constexpr int T = SPlan<N, E>::T;
     constexpr bool WS = (T <= 32);
     extern __shared__ float2 smem[];
@@ -53,28 +74,18 @@ __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
         for (int m = 0; m < E; ++m) v[m].y = -v[m].y;
     }
     fft_regs<N, E, WS>(v, t, buf, tw);
-    if (ok) {
-        float2* dst = out + (size_t)f * N + t;
-        if constexpr (INV) {
-            const float s = 1.0f / (float)N;
-#pragma unroll
-            for (int m = 0; m < E; ++m) __stcs(dst + m * T, make_float2(v[m].x * s, -v[m].y * s));
-        } else {
-#pragma unroll
-            for (int m = 0; m < E; ++m) __stcs(dst + m * T, v[m]);
-        }
-    }
+    if (ok) store_line<N, E, INV>(out + (size_t)f * N + t, v, adj);
 }
 
 template <int N, int E, int FPB, bool INV>
 static cudaError_t launch_batched(const float2* in, float2* out, long long batch, const float2* tw,
-                                  int*, cudaStream_t s) {
+                                  int*, cudaStream_t s, int adj) {
     constexpr int threads = SPlan<N, E>::T * FPB;
     constexpr int smem = FPB * spad_size(N) * (int)sizeof(float2);
     long long blocks = (batch + FPB - 1) / FPB;
     if (blocks <= 0) return cudaSuccess;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-    return launch_pdl(k_fft_batched<N, E, FPB, INV>, (unsigned)blocks, threads, smem, s, in, out, batch, tw);
+    return launch_pdl(k_fft_batched<N, E, FPB, INV>, (unsigned)blocks, threads, smem, s, in, out, batch, tw, adj);
 }
 
 template <class K>
@@ -105,7 +116,7 @@ static cudaError_t prepare_batched() {
 template <int N, int E, int FPB, int STAGES, bool INV>
 __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
     k_fft_stream(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
-                 const float2* __restrict__ tw, int* dev_err) {
+                 const float2* __restrict__ tw, int* dev_err, int adj) {
     constexpr int T = SPlan<N, E>::T;
     constexpr bool WS = (T <= 32);
     constexpr int STAGE = FPB * spad_size(N);  // float2 per stage buffer
@@ -142,10 +153,10 @@ __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
     for (long long g = blockIdx.x; g < groups; g += gridDim.x, ++it) {
         const int s = it % STAGES;
         const uint32_t parity = (uint32_t)((it / STAGES) & 1);
-        if (!mbar_wait(&full[s], parity)) {
-            report_device_error(dev_err, DEV_ERR_TMA_TIMEOUT);
-            return;
-        }
+        // Every thread waits (bounded) on its own; a thread that gives up still
+        // reaches the barrier below, which takes the decision for the whole CTA,
+        // so no thread leaves while another waits at a barrier.
+        const bool landed = mbar_wait(&full[s], parity);
         float2* buf = smem + s * STAGE;
         const long long f = g * FPB + lf;
         const bool ok = f < batch;
@@ -155,7 +166,20 @@ __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
             v[m] = ok ? buf[lf * N + t + m * T] : make_float2(0.f, 0.f);
             if constexpr (INV) v[m].y = -v[m].y;
         }
-        __syncthreads();  // the raw group is in registers; the buffer becomes the exchange area
+        // the raw group is in registers; the buffer becomes the exchange area
+        if (__syncthreads_or(!landed)) {
+            if (threadIdx.x == 0) {
+                report_device_error(dev_err, DEV_ERR_TMA_TIMEOUT);
+                // copies still in flight land before the CTA's shared memory goes away
+#pragma unroll
+                for (int d = 0; d < STAGES; ++d) {
+                    const int it2 = it + d;
+                    if (g + (long long)d * gridDim.x < groups)
+                        mbar_wait(&full[it2 % STAGES], (uint32_t)((it2 / STAGES) & 1));
+                }
+            }
+            return;
+        }
         fft_regs<N, E, WS>(v, t, PadLine{buf + lf * spad_size(N)}, tw);
         fence_proxy_async_smem();  // order this thread's exchange writes before the next bulk copy
         __syncthreads();           // every exchange access of this buffer is done
@@ -163,17 +187,7 @@ __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
             const long long gn = g + (long long)STAGES * gridDim.x;
             if (gn < groups) issue(gn, s);
         }
-        if (ok) {
-            float2* dst = out + (size_t)f * N + t;
-            if constexpr (INV) {
-                const float sc = 1.0f / (float)N;
-#pragma unroll
-                for (int m = 0; m < E; ++m) __stcs(dst + m * T, make_float2(v[m].x * sc, -v[m].y * sc));
-            } else {
-#pragma unroll
-                for (int m = 0; m < E; ++m) __stcs(dst + m * T, v[m]);
-            }
-        }
+        if (ok) store_line<N, E, INV>(out + (size_t)f * N + t, v, adj);
     }
 }
 
@@ -190,7 +204,7 @@ static int device_sms() {
 
 template <int N, int E, int FPB, int STAGES, bool INV>
 static cudaError_t launch_stream(const float2* in, float2* out, long long batch, const float2* tw,
-                                 int* dev_err, cudaStream_t s) {
+                                 int* dev_err, cudaStream_t s, int adj) {
     constexpr int threads = SPlan<N, E>::T * FPB;
     constexpr int smem = STAGES * FPB * spad_size(N) * (int)sizeof(float2);
     static int occ = 0;
@@ -204,7 +218,7 @@ static cudaError_t launch_stream(const float2* in, float2* out, long long batch,
     long long blocks = (long long)device_sms() * occ;
     if (blocks > groups) blocks = groups;
     return launch_pdl(k_fft_stream<N, E, FPB, STAGES, INV>, (unsigned)blocks, threads, smem, s, in, out, batch, tw,
-                      dev_err);
+                      dev_err, adj);
 }
 
 template <int N, int E, int FPB, int STAGES>

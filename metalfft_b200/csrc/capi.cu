@@ -312,15 +312,17 @@ extern "C" int64_t mfft_plan_size(const mfft_plan* plan) { return plan ? plan->n
 namespace mfft {
 
 int launch_c2c_device(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,
-                      cudaStream_t s) {
+                      cudaStream_t s, int adjoint) {
     cudaError_t e;
+    // the adjoint of one direction runs the other direction's kernel
+    const bool inv = (direction == MFFT_INVERSE) != (adjoint != 0);
     if (plan->n <= MFFT_MAX_SINGLE_N) {
         const BatchedKernel* k = plan->line.k;
-        e = (direction == MFFT_INVERSE ? k->inv : k->fwd)(in, out, batch, plan->line.tw, plan->ctx->dev_err, s);
+        e = (inv ? k->inv : k->fwd)(in, out, batch, plan->line.tw, plan->ctx->dev_err, s, adjoint);
         if (e != cudaSuccess) return cuda_error(e, "batched FFT launch");
         return MFFT_SUCCESS;
     }
-    return fourstep_exec(plan, in, out, batch, direction, s);
+    return fourstep_exec(plan, in, out, batch, inv ? MFFT_INVERSE : MFFT_FORWARD, s, adjoint);
 }
 
 int check_exec_args(const void* in, void* out, int64_t batch, int direction, int flags) {
@@ -512,6 +514,27 @@ extern "C" int mfft_exec_c2c(mfft_plan* plan, const void* in, void* out, int64_t
         plan->ctx, in, out, batch, line, line,
         [&](const void* di, void* dout, int64_t nl, cudaStream_t s) {
             return launch_c2c_device(plan, (const float2*)di, (float2*)dout, nl, direction, s);
+        },
+        true);
+}
+
+// Adjoint of mfft_exec_c2c (no reference counterpart): the same kernels with
+// the direction swapped and the 1/n scale moved to the other side.
+extern "C" int mfft_exec_c2c_backward(mfft_plan* plan, const void* grad_out, void* grad_in, int64_t batch,
+                                      int direction, int flags, void* stream) {
+    if (!plan) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "plan is NULL");
+    int st = check_exec_args(grad_out, grad_in, batch, direction, flags);
+    if (st) return st;
+    if (batch == 0) return MFFT_SUCCESS;
+    DeviceGuard g(plan->ctx->device);
+    if (flags == MFFT_DEVICE_MEMORY)
+        return launch_c2c_device(plan, (const float2*)grad_out, (float2*)grad_in, batch, direction,
+                                 (cudaStream_t)stream, 1);
+    const size_t line = (size_t)plan->n * sizeof(float2);
+    return run_host_lines(
+        plan->ctx, grad_out, grad_in, batch, line, line,
+        [&](const void* di, void* dout, int64_t nl, cudaStream_t s) {
+            return launch_c2c_device(plan, (const float2*)di, (float2*)dout, nl, direction, s, 1);
         },
         true);
 }

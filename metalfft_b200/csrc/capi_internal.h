@@ -85,8 +85,10 @@ int bind_batched(mfft_ctx* ctx, const BatchedKernel* k, BatchedBinding* b);
 const BatchedKernel* tuned_batched(mfft_ctx* ctx, int n);
 
 int check_exec_args(const void* in, void* out, int64_t batch, int direction, int flags);
+// adjoint = 1: the adjoint (conjugate transpose) of the transform in
+// `direction` instead of the transform (mfft_exec_c2c_backward)
 int launch_c2c_device(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,
-                      cudaStream_t s);
+                      cudaStream_t s, int adjoint = 0);
 int check_device_error(mfft_ctx* ctx);
 // Host-array call: copy in, run `body` on device buffers, copy out, wait.
 // in_place: the kernels may read and write one buffer (batched FFTs).
@@ -124,12 +126,12 @@ int fourstep_tables(mfft_ctx* ctx, int64_t n, float2** out);
 bool fsq_tma_size(int logn);
 struct FsqTables;
 int fourstep_tma_pass(int kind, const FsqTables& tabs, const float2* in, float2* out, float2* scratch, long long nb,
-                      int logn, bool inv, mfft_ctx* ctx, cudaStream_t s);
+                      int logn, bool inv, mfft_ctx* ctx, cudaStream_t s, int adjoint = 0);
 
 int fourstep_plan_init(mfft_plan* plan);
 void fourstep_plan_release(mfft_plan* plan);
 int fourstep_exec(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,
-                  cudaStream_t s);
+                  cudaStream_t s, int adjoint = 0);
 
 int tc_plan_init(mfft_plan* plan);
 void tc_plan_release(mfft_plan* plan);

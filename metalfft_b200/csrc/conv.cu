@@ -506,7 +506,7 @@ extern "C" int mfft_conv_create(mfft_ctx* ctx, const float* kernel, int64_t kern
         e = cudaMemcpyAsync(c->Dsum, hk.data(), sizeof(float2) * fft_size, cudaMemcpyHostToDevice, ctx->stream);
         if (e != cudaSuccess) st = cuda_error(e, "kernel upload");
         if (!st) {
-            e = bk->fwd(c->Dsum, c->H, 1, c->tw, ctx->dev_err, ctx->stream);
+            e = bk->fwd(c->Dsum, c->H, 1, c->tw, ctx->dev_err, ctx->stream, 0);
             if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
             if (e != cudaSuccess) st = cuda_error(e, "kernel spectrum");
         }

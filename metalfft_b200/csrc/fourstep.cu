@@ -130,7 +130,7 @@ static bool encode_rows(CUtensorMap* map, const float2* base, uint64_t rows, uin
 bool fsq_tma_size(int logn) { return logn >= 16 && logn <= 20; }
 
 int fourstep_tma_pass(int kind, const FsqTables& tabs, const float2* in, float2* out, float2* scratch, long long nb,
-                      int logn, bool inv, mfft_ctx* ctx, cudaStream_t s) {
+                      int logn, bool inv, mfft_ctx* ctx, cudaStream_t s, int adjoint) {
     int n1, n2;
     fsq_split(logn, &n1, &n2);
     FsqArgs a{};
@@ -138,6 +138,7 @@ int fourstep_tma_pass(int kind, const FsqTables& tabs, const float2* in, float2*
     a.out = out;
     a.scratch = scratch;
     a.u_logn = logn;
+    a.adjoint = adjoint;
     a.tabs = tabs;
     FsqMaps m{};
     bool ok;
@@ -158,13 +159,15 @@ int fourstep_tma_pass(int kind, const FsqTables& tabs, const float2* in, float2*
 
 // Column pass then row pass over chunks of up to scratch_lines transforms;
 // n = 2^16 .. 2^20 move their tiles with TMA (tile widths 4, 8 or 16).
-int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, int direction, cudaStream_t s) {
+int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, int direction, cudaStream_t s,
+                  int adjoint) {
     const FourStep& fs = p->fs;
     const int logn = ilog2c(p->n);
     const int nc = fsq_cols_items(logn), nr = fsq_rows_items(logn);
     FsqArgs a{};
     a.scratch = fs.scratch;
     a.u_logn = logn;
+    a.adjoint = adjoint;
     a.tabs.line_tw[ilog2c(fs.n1) - 6] = fs.col_tw;
     a.tabs.line_tw[ilog2c(fs.n2) - 6] = fs.row_tw;
     a.tabs.fine[logn - 13] = fs.tables;
@@ -175,8 +178,8 @@ int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, in
         a.in = in + b0 * p->n;
         a.out = out + b0 * p->n;
         if (fsq_tma_size(logn)) {
-            int st = fourstep_tma_pass(FSQ_COLS, a.tabs, a.in, a.out, a.scratch, nb, logn, inv, p->ctx, s);
-            if (!st) st = fourstep_tma_pass(FSQ_ROWS, a.tabs, a.in, a.out, a.scratch, nb, logn, inv, p->ctx, s);
+            int st = fourstep_tma_pass(FSQ_COLS, a.tabs, a.in, a.out, a.scratch, nb, logn, inv, p->ctx, s, adjoint);
+            if (!st) st = fourstep_tma_pass(FSQ_ROWS, a.tabs, a.in, a.out, a.scratch, nb, logn, inv, p->ctx, s, adjoint);
             if (st) return st;
             continue;
         }

@@ -101,9 +101,16 @@ __device__ __forceinline__ void load_linear(float2* st, const float2* g, int cou
 
 // ---- the three item kinds ---------------------------------------------------
 
+// Output scale of a transform of n points: the inverse is scaled by 1/n, the
+// forward is not; the adjoint swaps the two (both scalings are exact).
+template <bool INV>
+__device__ __forceinline__ float out_scale(long long n, int adj) {
+    return (INV != (adj != 0)) ? 1.0f / (float)n : 1.0f;
+}
+
 template <int L, bool INV>
 __device__ __forceinline__ void do_lines(float2* st, float2* __restrict__ out, long long off, int lines,
-                                         const float2* __restrict__ tw) {
+                                         const float2* __restrict__ tw, float s) {
     constexpr int T = L / 16;
     const int u = threadIdx.x / T, t = threadIdx.x % T;
     float2 v[16];
@@ -116,9 +123,8 @@ __device__ __forceinline__ void do_lines(float2* st, float2* __restrict__ out, l
     fft_regs<L, 16, (T <= 32)>(v, t, PadLine{st + u * spad_size(L)}, tw);
     if (u < lines) {
         float2* dst = out + off + (long long)u * L + t;
-        const float s = 1.0f / (float)L;
 #pragma unroll
-        for (int m = 0; m < 16; ++m) __stcs(dst + m * T, INV ? make_float2(v[m].x * s, -v[m].y * s) : v[m]);
+        for (int m = 0; m < 16; ++m) __stcs(dst + m * T, make_float2(v[m].x * s, INV ? -v[m].y * s : v[m].y * s));
     }
 }
 
@@ -188,7 +194,7 @@ __device__ __forceinline__ void do_rows(float2* st, const float2* mid_rows, floa
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < 16; ++m)
-        st[tidx(t + m * T, r, LR)] = INV ? make_float2(v[m].x * scale, -v[m].y * scale) : v[m];
+        st[tidx(t + m * T, r, LR)] = make_float2(v[m].x * scale, INV ? -v[m].y * scale : v[m].y * scale);
     if constexpr (!TILE_OUT) {
         __syncthreads();
         store_tile<true>(st, out + row0, LL, LR, 1LL << ln1);
@@ -249,14 +255,15 @@ template <bool INV, bool TILE_OUT = false>
 __device__ __forceinline__ void compute(const FsqArgs& a, const Work& w, float2* st) {
     if (w.kind == FSQ_LINES) {
         const float2* tw = a.tabs.line_tw[w.logn - 6];
+        const float s = out_scale<INV>(1LL << w.logn, a.adjoint);
         switch (w.logn) {
-            case 6: do_lines<64, INV>(st, a.out, w.off, w.lines, tw); break;
-            case 7: do_lines<128, INV>(st, a.out, w.off, w.lines, tw); break;
-            case 8: do_lines<256, INV>(st, a.out, w.off, w.lines, tw); break;
-            case 9: do_lines<512, INV>(st, a.out, w.off, w.lines, tw); break;
-            case 10: do_lines<1024, INV>(st, a.out, w.off, w.lines, tw); break;
-            case 11: do_lines<2048, INV>(st, a.out, w.off, w.lines, tw); break;
-            default: do_lines<4096, INV>(st, a.out, w.off, w.lines, tw); break;
+            case 6: do_lines<64, INV>(st, a.out, w.off, w.lines, tw, s); break;
+            case 7: do_lines<128, INV>(st, a.out, w.off, w.lines, tw, s); break;
+            case 8: do_lines<256, INV>(st, a.out, w.off, w.lines, tw, s); break;
+            case 9: do_lines<512, INV>(st, a.out, w.off, w.lines, tw, s); break;
+            case 10: do_lines<1024, INV>(st, a.out, w.off, w.lines, tw, s); break;
+            case 11: do_lines<2048, INV>(st, a.out, w.off, w.lines, tw, s); break;
+            default: do_lines<4096, INV>(st, a.out, w.off, w.lines, tw, s); break;
         }
         return;
     }
@@ -279,7 +286,7 @@ __device__ __forceinline__ void compute(const FsqArgs& a, const Work& w, float2*
         const int row0 = w.index << (ilog2c(FSQ_POINTS) - l2);
         const float2* rows = mid + ((long long)row0 << l2);
         float2* dst = a.out + w.off;
-        const float scale = 1.0f / (float)(1LL << w.logn);
+        const float scale = out_scale<INV>(1LL << w.logn, a.adjoint);
         switch (l2) {
             case 7: do_rows<128, INV, TILE_OUT>(st, rows, dst, l1, row0, tw, scale); break;
             case 8: do_rows<256, INV, TILE_OUT>(st, rows, dst, l1, row0, tw, scale); break;

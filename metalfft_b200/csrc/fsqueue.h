@@ -63,6 +63,9 @@ struct FsqArgs {
     // points: u_kind FSQ_COLS (pass 0) or FSQ_ROWS (pass 1), u_per items each;
     // transform j's intermediate is scratch + j * 2^u_logn
     int u_kind, u_logn, u_per;
+    // 1: the adjoint of the transform (the inverse unscaled, the forward
+    // scaled by 1/n); 0: the transform
+    int adjoint;
     FsqTables tabs;
 };
 

@@ -6,8 +6,12 @@
 
 namespace mfft {
 
+// adjoint = 0: the transform itself (forward unscaled, inverse scaled by 1/N);
+// adjoint = 1: its adjoint (conjugate transpose) -- the inverse kernel unscaled
+// (adjoint of the forward) or the forward kernel scaled by 1/N (adjoint of
+// the inverse), the scaling fused into the store.
 typedef cudaError_t (*batched_launch_fn)(const float2* in, float2* out, long long batch,
-                                         const float2* tw, int* dev_err, cudaStream_t s);
+                                         const float2* tw, int* dev_err, cudaStream_t s, int adjoint);
 
 // One instantiation of the batched in-shared-memory FFT.
 struct BatchedKernel {

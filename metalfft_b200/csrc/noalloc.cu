@@ -18,6 +18,9 @@
 // every element the row pass reads), but two calls that overlap on the GPU
 // (different streams, or different host threads) race on the intermediate:
 // serialise them.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <mutex>
 
 #include "capi_internal.h"
@@ -39,6 +42,7 @@ static __device__ __align__(256) float2 g_noalloc_coarse[NA_SIZES][NA_FINE];
 
 struct NoallocDevice {
     bool ready = false;
+    unsigned long long ctx_id = 0;  // the CUDA context the addresses and tables belong to
     float2* scratch = nullptr;
     float2* line_tw = nullptr;
     float2* fine = nullptr;
@@ -48,6 +52,20 @@ std::mutex g_noalloc_mu;
 NoallocDevice g_noalloc_dev[64];
 
 __host__ __device__ constexpr int na_tile_cols(int L) { return L >= 1024 ? 8 : NA_TILE; }
+
+// Every launch of this file goes through here and is checked as it is made:
+// the status is this launch's own, so an earlier error of unrelated code is
+// neither reported as ours nor cleared.
+template <class... KArgs, class... Args>
+cudaError_t na_launch(void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                      Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    return cudaLaunchKernelEx(&cfg, k, (KArgs)args...);
+}
 
 __global__ void k_na_line_rows(float2* tw, int off, int ns, int radix, int rowlen) {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -72,14 +90,16 @@ __global__ void k_na_tables(float2* fine, float2* coarse, int n) {
 }
 
 template <int L>
-void na_gen_line(float2* tw, cudaStream_t s) {
+cudaError_t na_gen_line(float2* tw, cudaStream_t s) {
     using PL = SPlan<L, 16>;
     static_assert(PL::TWSIZE <= NA_LINE_TW, "line twiddle slot too small");
     for (int p = 1; p < PL::NPASS; ++p) {
         int cnt = PL::span(p) * PL::twrow(PL::radix(p));
-        k_na_line_rows<<<(cnt + 255) / 256, 256, 0, s>>>(tw, PL::twoff(p), PL::span(p), PL::radix(p),
-                                                         PL::twrow(PL::radix(p)));
+        cudaError_t e = na_launch(k_na_line_rows, (unsigned)((cnt + 255) / 256), 256u, 0, s, tw, PL::twoff(p),
+                                  PL::span(p), PL::radix(p), PL::twrow(PL::radix(p)));
+        if (e != cudaSuccess) return e;
     }
+    return cudaSuccess;
 }
 
 // column pass: C columns per CTA, FFT of length L down each column, times
@@ -166,33 +186,74 @@ cudaError_t na_prepare() {
 }
 
 template <int L>
-void na_cols(const float2* in, float2* mid, int n2, const float2* tw, const float2* fine, const float2* coarse,
-             long long nb, bool inv, cudaStream_t s) {
+cudaError_t na_cols(const float2* in, float2* mid, int n2, const float2* tw, const float2* fine,
+                    const float2* coarse, long long nb, bool inv, cudaStream_t s) {
     constexpr int C = na_tile_cols(L);
     const size_t smem = (size_t)L * C * sizeof(float2);
     const unsigned blocks = (unsigned)(nb * (n2 / C));
-    if (inv) k_na_cols<L, true><<<blocks, L / 16 * C, smem, s>>>(in, mid, n2, tw, fine, coarse);
-    else k_na_cols<L, false><<<blocks, L / 16 * C, smem, s>>>(in, mid, n2, tw, fine, coarse);
+    return inv ? na_launch(k_na_cols<L, true>, blocks, (unsigned)(L / 16 * C), smem, s, in, mid, n2, tw, fine, coarse)
+               : na_launch(k_na_cols<L, false>, blocks, (unsigned)(L / 16 * C), smem, s, in, mid, n2, tw, fine, coarse);
 }
 
 template <int L>
-void na_rows(const float2* mid, float2* out, int n1, const float2* tw, long long nb, bool inv, cudaStream_t s) {
+cudaError_t na_rows(const float2* mid, float2* out, int n1, const float2* tw, long long nb, bool inv,
+                    cudaStream_t s) {
     const size_t smem = (size_t)L * NA_TILE * sizeof(float2);
     const unsigned blocks = (unsigned)(nb * (n1 / NA_TILE));
-    if (inv) k_na_rows<L, true><<<blocks, L, smem, s>>>(mid, out, n1, tw);
-    else k_na_rows<L, false><<<blocks, L, smem, s>>>(mid, out, n1, tw);
+    return inv ? na_launch(k_na_rows<L, true>, blocks, (unsigned)L, smem, s, mid, out, n1, tw)
+               : na_launch(k_na_rows<L, false>, blocks, (unsigned)L, smem, s, mid, out, n1, tw);
 }
 
-// Once per device, with that device current: resolve the arrays' device
-// addresses (cudaGetSymbolAddress), fill the tables and raise the kernels'
-// shared-memory limits.  Launches kernels but allocates nothing.
+// Unique id of the calling thread's current CUDA context (the device's primary
+// context, made current if no context is).  A device reset destroys the
+// primary context; the next one gets a new id, so the set-up below is redone
+// for it instead of reusing addresses and tables of the old context.
+// (driver entry points through the runtime: the library has no link-time
+// dependency on the driver library)
+int na_context_id(int dev, unsigned long long* id) {
+    static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(f);
+    });
+    if (!get_current || !get_id)
+        return set_error(MFFT_ERR_NO_DEVICE, -1, -1, -1, "no-alloc set-up: driver context queries unavailable");
+    CUcontext c = nullptr;
+    if (get_current(&c) != CUDA_SUCCESS || !c) {
+        cudaError_t e = cudaSetDevice(dev);  // initialises and binds the primary context
+        if (e != cudaSuccess) return cuda_error(e, "no-alloc set-up: cudaSetDevice");
+        if (get_current(&c) != CUDA_SUCCESS || !c)
+            return set_error(MFFT_ERR_NO_DEVICE, -1, -1, -1, "no-alloc set-up: no current CUDA context");
+    }
+    if (get_id(c, id) != CUDA_SUCCESS)
+        return set_error(MFFT_ERR_NO_DEVICE, -1, -1, -1, "no-alloc set-up: cuCtxGetId failed");
+    return MFFT_SUCCESS;
+}
+
+// Once per device (and again after a device reset), with that device
+// current: resolve the arrays' device addresses (cudaGetSymbolAddress), fill
+// the tables and raise the kernels' shared-memory limits.  Launches kernels
+// but allocates nothing.
 int na_setup(int dev, cudaStream_t s, NoallocDevice** out) {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     NoallocDevice& d = g_noalloc_dev[dev];
-    if (d.ready) {
+    unsigned long long id = 0;
+    int st = na_context_id(dev, &id);
+    if (st) return st;
+    if (d.ready && d.ctx_id == id) {
         *out = &d;
         return MFFT_SUCCESS;
     }
+    d.ready = false;
     cudaError_t e = cudaGetSymbolAddress((void**)&d.scratch, g_noalloc_scratch);
     if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&d.line_tw, g_noalloc_line_tw);
     if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&d.fine, g_noalloc_fine);
@@ -201,15 +262,17 @@ int na_setup(int dev, cudaStream_t s, NoallocDevice** out) {
     if ((e = na_prepare<128>()) || (e = na_prepare<256>()) || (e = na_prepare<512>()) ||
         (e = na_prepare<1024>()))
         return cuda_error(e, "no-alloc set-up: kernel attributes");
-    na_gen_line<128>(d.line_tw + 0 * NA_LINE_TW, s);
-    na_gen_line<256>(d.line_tw + 1 * NA_LINE_TW, s);
-    na_gen_line<512>(d.line_tw + 2 * NA_LINE_TW, s);
-    na_gen_line<1024>(d.line_tw + 3 * NA_LINE_TW, s);
-    for (int i = 0; i < NA_SIZES; ++i)
-        k_na_tables<<<(NA_FINE + 255) / 256, 256, 0, s>>>(d.fine + i * NA_FINE, d.coarse + i * NA_FINE, 1 << (15 + i));
+    if ((e = na_gen_line<128>(d.line_tw + 0 * NA_LINE_TW, s)) || (e = na_gen_line<256>(d.line_tw + 1 * NA_LINE_TW, s)) ||
+        (e = na_gen_line<512>(d.line_tw + 2 * NA_LINE_TW, s)) || (e = na_gen_line<1024>(d.line_tw + 3 * NA_LINE_TW, s)))
+        return cuda_error(e, "no-alloc set-up: twiddle launch");
+    for (int i = 0; i < NA_SIZES; ++i) {
+        e = na_launch(k_na_tables, (unsigned)((NA_FINE + 255) / 256), 256u, 0, s, d.fine + i * NA_FINE,
+                      d.coarse + i * NA_FINE, 1 << (15 + i));
+        if (e != cudaSuccess) return cuda_error(e, "no-alloc set-up: twiddle launch");
+    }
     e = cudaStreamSynchronize(s);
-    if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "no-alloc set-up: tables");
+    d.ctx_id = id;
     d.ready = true;
     *out = &d;
     return MFFT_SUCCESS;
@@ -223,7 +286,8 @@ int na_line_slot(int L) { return L == 128 ? 0 : L == 256 ? 1 : L == 512 ? 2 : 3;
 // Four-step C2C FFT of `batch` lines of length n (a power of two from 2^15 to
 // 2^20) on device memory, enqueued on `stream`; no device memory is allocated.
 // The first call on a device does a one-time set-up that launches kernels and
-// waits for them: make that first call before any stream capture begins.
+// waits for them: make that first call before any stream capture begins.  The
+// set-up is redone on the first call after a device reset.
 extern "C" int mfft_fourstep_noalloc(const void* in, void* out, int64_t n, int64_t batch, int direction,
                                      void* stream) {
     using namespace mfft;
@@ -259,18 +323,18 @@ extern "C" int mfft_fourstep_noalloc(const void* in, void* out, int64_t n, int64
     for (int64_t b0 = 0; b0 < batch; b0 += chunk) {
         const long long nb = batch - b0 < chunk ? batch - b0 : chunk;
         switch (n1) {
-            case 128: na_cols<128>(x + b0 * n, d->scratch, n2, ctw, fine, coarse, nb, inv, s); break;
-            case 256: na_cols<256>(x + b0 * n, d->scratch, n2, ctw, fine, coarse, nb, inv, s); break;
-            case 512: na_cols<512>(x + b0 * n, d->scratch, n2, ctw, fine, coarse, nb, inv, s); break;
-            default: na_cols<1024>(x + b0 * n, d->scratch, n2, ctw, fine, coarse, nb, inv, s); break;
+            case 128: e = na_cols<128>(x + b0 * n, d->scratch, n2, ctw, fine, coarse, nb, inv, s); break;
+            case 256: e = na_cols<256>(x + b0 * n, d->scratch, n2, ctw, fine, coarse, nb, inv, s); break;
+            case 512: e = na_cols<512>(x + b0 * n, d->scratch, n2, ctw, fine, coarse, nb, inv, s); break;
+            default: e = na_cols<1024>(x + b0 * n, d->scratch, n2, ctw, fine, coarse, nb, inv, s); break;
         }
+        if (e != cudaSuccess) return cuda_error(e, "mfft_fourstep_noalloc column-pass launch");
         switch (n2) {
-            case 256: na_rows<256>(d->scratch, y + b0 * n, n1, rtw, nb, inv, s); break;
-            case 512: na_rows<512>(d->scratch, y + b0 * n, n1, rtw, nb, inv, s); break;
-            default: na_rows<1024>(d->scratch, y + b0 * n, n1, rtw, nb, inv, s); break;
+            case 256: e = na_rows<256>(d->scratch, y + b0 * n, n1, rtw, nb, inv, s); break;
+            case 512: e = na_rows<512>(d->scratch, y + b0 * n, n1, rtw, nb, inv, s); break;
+            default: e = na_rows<1024>(d->scratch, y + b0 * n, n1, rtw, nb, inv, s); break;
         }
+        if (e != cudaSuccess) return cuda_error(e, "mfft_fourstep_noalloc row-pass launch");
     }
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_error(e, "mfft_fourstep_noalloc launch");
     return MFFT_SUCCESS;
 }

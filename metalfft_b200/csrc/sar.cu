@@ -22,6 +22,9 @@
 //                         (one more FFT on the registers), per-tile partials
 //                         of dphi_p = -sum_r Im(u_p[r] conj(B[p][r]))
 //   reduce  k_sar_reduce  partials summed over tiles in a fixed order (FP64)
+// The range-compressed intermediate between the passes is FP16 with per-pulse
+// scales by default; mfft_sar_set_intermediate switches it to FP32 (no
+// scales), which the phase adjoint needs to meet FP64 gradients to ~1e-5.
 #include <cuda_fp16.h>
 
 #include <vector>
@@ -202,11 +205,16 @@ __global__ void k_sar_quantize(const float2* __restrict__ raw, long long nr, __h
     if (threadIdx.x == 0) scale[p] = s;
 }
 
-// pass A: range compression of one pulse per CTA
-template <int NR>
+// the range-compressed intermediate: FP16 (times a per-pulse scale) or FP32
+__device__ __forceinline__ float2 ld_rc(const __half2* p) { return __half22float2(*p); }
+__device__ __forceinline__ float2 ld_rc(const float2* p) { return *p; }
+
+// pass A: range compression of one pulse per CTA; RC = __half2 (FP16 with a
+// per-pulse scale) or float2 (FP32, scale 1)
+template <int NR, class RC>
 __global__ void __launch_bounds__(NR / SAR_E) k_sar_range(const __half2* __restrict__ raw, const float* __restrict__ pscale,
                                                            const float* __restrict__ phase, const float2* __restrict__ H,
-                                                           const float2* __restrict__ tw, __half2* __restrict__ rc,
+                                                           const float2* __restrict__ tw, RC* __restrict__ rc,
                                                            float* __restrict__ rc_scale) {
     constexpr int T = NR / SAR_E;
     extern __shared__ __align__(16) float2 smem[];
@@ -232,12 +240,18 @@ __global__ void __launch_bounds__(NR / SAR_E) k_sar_range(const __half2* __restr
         v[m] = make_float2(v[m].x * inv_n, -v[m].y * inv_n);
         mx = fmaxf(mx, fmaxf(fabsf(v[m].x), fabsf(v[m].y)));
     }
-    const float s = block_scale(cta_max(mx, red));
-    const float inv = 1.f / s;
-    __half2* rcp = rc + p * NR + t;
+    RC* rcp = rc + p * NR + t;
+    if constexpr (sizeof(RC) == sizeof(float2)) {
 #pragma unroll
-    for (int m = 0; m < SAR_E; ++m) rcp[m * T] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
-    if (t == 0) rc_scale[p] = s;
+        for (int m = 0; m < SAR_E; ++m) rcp[m * T] = v[m];
+        if (t == 0) rc_scale[p] = 1.f;
+    } else {
+        const float s = block_scale(cta_max(mx, red));
+        const float inv = 1.f / s;
+#pragma unroll
+        for (int m = 0; m < SAR_E; ++m) rcp[m * T] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
+        if (t == 0) rc_scale[p] = s;
+    }
 }
 
 template <int NA>
@@ -249,9 +263,9 @@ struct AzGeom {
 
 // pass B: azimuth FFT of C range columns; IMAGE: write the FP16 image;
 // GRAD: per-tile partials of dL/dphi and of L = sum |I|^4
-template <int NA, bool IMAGE, bool GRAD, bool INV = false>
+template <int NA, bool IMAGE, bool GRAD, bool INV = false, class RC = __half2>
 __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
-    k_sar_azimuth(const __half2* __restrict__ rc, const float* __restrict__ rc_scale, long long nr,
+    k_sar_azimuth(const RC* __restrict__ rc, const float* __restrict__ rc_scale, long long nr,
                   const float2* __restrict__ tw, __half2* __restrict__ image, float* __restrict__ image_scale,
                   float* __restrict__ dphi_part, double* __restrict__ loss_part) {
     constexpr int T = AzGeom<NA>::T, C = AzGeom<NA>::C;
@@ -262,13 +276,13 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
     const int c = threadIdx.x % C, t = threadIdx.x / C;
     const long long col = tile * C + c;
     // rows t + m*T of column col: a base pointer and a stride of T rows
-    const __half2* rcol = rc + (long long)t * nr + col;
+    const RC* rcol = rc + (long long)t * nr + col;
     const long long rstep = (long long)T * nr;
     float2 v[SAR_E];
 #pragma unroll
     for (int m = 0; m < SAR_E; ++m) {
         const int p = t + m * T;
-        const float2 u = __half22float2(rcol[m * rstep]);
+        const float2 u = ld_rc(rcol + m * rstep);
         const float s = __ldg(rc_scale + p);
         v[m] = make_float2(u.x * s, INV ? -u.y * s : u.y * s);
     }
@@ -312,7 +326,7 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
 #pragma unroll
         for (int m = 0; m < SAR_E; ++m) {
             const int p = t + m * T;
-            const float2 u0 = __half22float2(rcol[m * rstep]);
+            const float2 u0 = ld_rc(rcol + m * rstep);
             const float s = __ldg(rc_scale + p);
             const float2 u = make_float2(u0.x * s, u0.y * s);
             // -Im(u conj(B)) with v = conj(B): -Im(u v)
@@ -483,55 +497,70 @@ void l_rcmc(int grid, cudaStream_t s, const __half2* rd, const float* rds, const
     k_sar_rcmc<NR><<<grid, NR / SAR_E, NR * 8, s>>>(rd, rds, rows, out, outs);
 }
 
-typedef void (*range_fn)(int grid, cudaStream_t, const __half2*, const float*, const float*, const float2*,
-                         const float2*, __half2*, float*);
-typedef void (*az_fn)(int grid, cudaStream_t, const __half2*, const float*, long long, const float2*, __half2*, float*,
-                      float*, double*);
+template <class RC>
+using range_fn_t = void (*)(int grid, cudaStream_t, const __half2*, const float*, const float*, const float2*,
+                            const float2*, RC*, float*);
+template <class RC>
+using az_fn_t = void (*)(int grid, cudaStream_t, const RC*, const float*, long long, const float2*, __half2*, float*,
+                         float*, double*);
+typedef az_fn_t<__half2> az_fn;
 
-template <int NR>
+template <int NR, class RC>
 void l_range(int grid, cudaStream_t s, const __half2* raw, const float* ps, const float* ph, const float2* H,
-             const float2* tw, __half2* rc, float* rcs) {
-    k_sar_range<NR><<<grid, NR / SAR_E, spad_size(NR) * 8, s>>>(raw, ps, ph, H, tw, rc, rcs);
+             const float2* tw, RC* rc, float* rcs) {
+    k_sar_range<NR, RC><<<grid, NR / SAR_E, spad_size(NR) * 8, s>>>(raw, ps, ph, H, tw, rc, rcs);
 }
-template <int NA, bool IMAGE, bool GRAD, bool INV = false>
-void l_az(int grid, cudaStream_t s, const __half2* rc, const float* rcs, long long nr, const float2* tw, __half2* img,
+template <int NA, bool IMAGE, bool GRAD, bool INV = false, class RC = __half2>
+void l_az(int grid, cudaStream_t s, const RC* rc, const float* rcs, long long nr, const float2* tw, __half2* img,
           float* imgs, float* dp, double* lp) {
-    k_sar_azimuth<NA, IMAGE, GRAD, INV><<<grid, AzGeom<NA>::THREADS, NA * AzGeom<NA>::C * 8, s>>>(rc, rcs, nr, tw, img,
-                                                                                                 imgs, dp, lp);
+    k_sar_azimuth<NA, IMAGE, GRAD, INV, RC><<<grid, AzGeom<NA>::THREADS, NA * AzGeom<NA>::C * 8, s>>>(
+        rc, rcs, nr, tw, img, imgs, dp, lp);
 }
 template <int NR>
 cudaError_t prep_range() {
-    cudaError_t e = cudaFuncSetAttribute(k_sar_range<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, spad_size(NR) * 8);
+    const int sm = spad_size(NR) * 8;
+    cudaError_t e = cudaFuncSetAttribute(k_sar_range<NR, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_sar_range<NR, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_sar_rcmc<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, NR * 8);
 }
+template <int NA, bool IMAGE, bool GRAD, bool INV, class RC>
+cudaError_t prep_az1() {
+    return cudaFuncSetAttribute(k_sar_azimuth<NA, IMAGE, GRAD, INV, RC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                NA * AzGeom<NA>::C * 8);
+}
 template <int NA>
 cudaError_t prep_az() {
-    const int sm = NA * AzGeom<NA>::C * 8;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_sar_azimuth<NA, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    if ((e = cudaFuncSetAttribute(k_sar_azimuth<NA, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-    if ((e = cudaFuncSetAttribute(k_sar_azimuth<NA, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm)))
-        return e;
-    return cudaFuncSetAttribute(k_sar_azimuth<NA, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if ((e = prep_az1<NA, true, false, false, __half2>())) return e;
+    if ((e = prep_az1<NA, false, true, false, __half2>())) return e;
+    if ((e = prep_az1<NA, true, false, true, __half2>())) return e;
+    if ((e = prep_az1<NA, true, true, false, __half2>())) return e;
+    if ((e = prep_az1<NA, true, false, false, float2>())) return e;
+    if ((e = prep_az1<NA, false, true, false, float2>())) return e;
+    return prep_az1<NA, true, true, false, float2>();
 }
 
 struct RangeK {
     int n;
-    range_fn f;
+    range_fn_t<__half2> f;
+    range_fn_t<float2> f32;
     cudaError_t (*prep)();
     rcmc_fn rcmc;
 };
 struct AzK {
     int n, cols;
     az_fn fwd, bwd, both, inv;
+    az_fn_t<float2> fwd32, bwd32, both32;
     cudaError_t (*prep)();
 };
-#define MFFT_RANGE(N) {N, &l_range<N>, &prep_range<N>, &l_rcmc<N>}
+#define MFFT_RANGE(N) {N, &l_range<N, __half2>, &l_range<N, float2>, &prep_range<N>, &l_rcmc<N>}
 const RangeK g_range[] = {MFFT_RANGE(512),  MFFT_RANGE(1024), MFFT_RANGE(2048),
                           MFFT_RANGE(4096), MFFT_RANGE(8192), MFFT_RANGE(16384)};
 #define MFFT_AZ(N)                                                                                              \
     {N, AzGeom<N>::C, &l_az<N, true, false>, &l_az<N, false, true>, &l_az<N, true, true>, &l_az<N, true, false, true>, \
+     &l_az<N, true, false, false, float2>, &l_az<N, false, true, false, float2>, &l_az<N, true, true, false, float2>, \
      &prep_az<N>}
 const AzK g_az[] = {MFFT_AZ(64), MFFT_AZ(128), MFFT_AZ(256), MFFT_AZ(512), MFFT_AZ(1024), MFFT_AZ(2048), MFFT_AZ(4096)};
 
@@ -557,12 +586,14 @@ struct mfft_sar {
     float2* tw_a = nullptr;
     float2* H = nullptr;
     __half2* rc = nullptr;  // range-compressed pulses, FP16 pulse-major
+    float2* rc32 = nullptr; // the same in FP32 (allocated when selected)
+    int rc_fp32 = 0;        // MFFT_SAR_RC_FP16 / MFFT_SAR_RC_FP32
     float* rc_scale = nullptr;
     float* dphi_part = nullptr;
     double* loss_part = nullptr;
     long long tiles = 0;
     cudaGraphExec_t graph = nullptr;
-    const void* g_key[8] = {};
+    const void* g_key[9] = {};
     // focusing (allocated by the first mfft_sar_focus)
     __half2* rd2 = nullptr;      // RCMC'd, matched-filtered rows, FP16
     float* rd2_scale = nullptr;  // one scale per Doppler row
@@ -671,6 +702,7 @@ extern "C" int mfft_sar_destroy(mfft_sar* s) {
     if (s->graph) cudaGraphExecDestroy(s->graph);
     cudaFree(s->H);
     cudaFree(s->rc);
+    cudaFree(s->rc32);
     cudaFree(s->rc_scale);
     cudaFree(s->dphi_part);
     cudaFree(s->loss_part);
@@ -728,7 +760,7 @@ extern "C" int mfft_sar_create(mfft_ctx* ctx, const mfft_sar_params* p, const vo
         memcpy(h.data(), chirp_ref, sizeof(float2) * nr);
         float2* tmp = s->H + nr;
         e = cudaMemcpyAsync(tmp, h.data(), sizeof(float2) * nr, cudaMemcpyHostToDevice, ctx->stream);
-        if (e == cudaSuccess) e = br.k->fwd(tmp, s->H, 1, br.tw, ctx->dev_err, ctx->stream);
+        if (e == cudaSuccess) e = br.k->fwd(tmp, s->H, 1, br.tw, ctx->dev_err, ctx->stream, 0);
         if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), s->H, sizeof(float2) * nr, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         for (auto& v : h) v.y = -v.y;
@@ -744,7 +776,40 @@ extern "C" int mfft_sar_create(mfft_ctx* ctx, const mfft_sar_params* p, const vo
 }
 
 static int sar_pass_a(mfft_sar* s, const void* raw_h, const float* ps, const float* ph, cudaStream_t st) {
-    s->rk->f((int)s->prm.pulses, st, (const __half2*)raw_h, ps, ph, s->H, s->tw_r, s->rc, s->rc_scale);
+    if (s->rc_fp32)
+        s->rk->f32((int)s->prm.pulses, st, (const __half2*)raw_h, ps, ph, s->H, s->tw_r, s->rc32, s->rc_scale);
+    else
+        s->rk->f((int)s->prm.pulses, st, (const __half2*)raw_h, ps, ph, s->H, s->tw_r, s->rc, s->rc_scale);
+    return MFFT_SUCCESS;
+}
+
+// pass B in the selected intermediate precision: which = 0 image, 1 adjoint, 2 both
+static void sar_pass_b(mfft_sar* s, int which, cudaStream_t st, void* image_h, float* image_scale) {
+    const long long nr = s->prm.range_n;
+    const int tiles = (int)s->tiles;
+    if (s->rc_fp32) {
+        const az_fn_t<float2> f = which == 0 ? s->ak->fwd32 : which == 1 ? s->ak->bwd32 : s->ak->both32;
+        f(tiles, st, s->rc32, s->rc_scale, nr, s->tw_a, (__half2*)image_h, image_scale, s->dphi_part, s->loss_part);
+    } else {
+        const az_fn f = which == 0 ? s->ak->fwd : which == 1 ? s->ak->bwd : s->ak->both;
+        f(tiles, st, s->rc, s->rc_scale, nr, s->tw_a, (__half2*)image_h, image_scale, s->dphi_part, s->loss_part);
+    }
+}
+
+extern "C" int mfft_sar_set_intermediate(mfft_sar* s, int precision) {
+    if (!s) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "sar is NULL");
+    if (precision != MFFT_SAR_RC_FP16 && precision != MFFT_SAR_RC_FP32)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, precision, -1, "unknown SAR intermediate precision %d",
+                         precision);
+    if (precision == MFFT_SAR_RC_FP32 && !s->rc32) {
+        DeviceGuard gd(s->ctx->device);
+        cudaError_t e = cudaMalloc(&s->rc32, sizeof(float2) * (size_t)s->prm.pulses * (size_t)s->prm.range_n);
+        if (e != cudaSuccess) {
+            s->rc32 = nullptr;
+            return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "SAR FP32 intermediate: %s", cudaGetErrorString(e));
+        }
+    }
+    s->rc_fp32 = precision == MFFT_SAR_RC_FP32;
     return MFFT_SUCCESS;
 }
 
@@ -760,8 +825,7 @@ extern "C" int mfft_sar_forward(mfft_sar* s, const void* raw_h, const float* pul
     DeviceGuard gd(s->ctx->device);
     cudaStream_t st = (cudaStream_t)stream;
     sar_pass_a(s, raw_h, pulse_scale, phase, st);
-    s->ak->fwd((int)s->tiles, st, s->rc, s->rc_scale, s->prm.range_n, s->tw_a, (__half2*)image_h, image_scale, nullptr,
-               nullptr);
+    sar_pass_b(s, 0, st, image_h, image_scale);
     return sar_check_launch("SAR forward");
 }
 
@@ -772,8 +836,7 @@ extern "C" int mfft_sar_backward_phase(mfft_sar* s, const void* raw_h, const flo
     DeviceGuard gd(s->ctx->device);
     cudaStream_t st = (cudaStream_t)stream;
     sar_pass_a(s, raw_h, pulse_scale, phase, st);
-    s->ak->bwd((int)s->tiles, st, s->rc, s->rc_scale, s->prm.range_n, s->tw_a, nullptr, nullptr, s->dphi_part,
-               s->loss_part);
+    sar_pass_b(s, 1, st, nullptr, nullptr);
     k_sar_reduce<<<(unsigned)((s->prm.pulses + 31) / 32 + 1), SAR_RED_THREADS, 0, st>>>(
         s->dphi_part, s->tiles, s->prm.pulses, dphi, s->loss_part, loss);
     return sar_check_launch("SAR backward");
@@ -782,8 +845,7 @@ extern "C" int mfft_sar_backward_phase(mfft_sar* s, const void* raw_h, const flo
 static void sar_enqueue_step(mfft_sar* s, const void* raw_h, const float* ps, const float* ph, void* image_h,
                              float* image_scale, float* dphi, double* loss, cudaStream_t st) {
     sar_pass_a(s, raw_h, ps, ph, st);
-    s->ak->both((int)s->tiles, st, s->rc, s->rc_scale, s->prm.range_n, s->tw_a, (__half2*)image_h, image_scale,
-                s->dphi_part, s->loss_part);
+    sar_pass_b(s, 2, st, image_h, image_scale);
     k_sar_reduce<<<(unsigned)((s->prm.pulses + 31) / 32 + 1), SAR_RED_THREADS, 0, st>>>(
         s->dphi_part, s->tiles, s->prm.pulses, dphi, s->loss_part, loss);
 }
@@ -794,9 +856,10 @@ extern "C" int mfft_sar_step_graph(mfft_sar* s, const void* raw_h, const float* 
         return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "NULL argument");
     DeviceGuard gd(s->ctx->device);
     cudaStream_t st = (cudaStream_t)stream;
-    const void* key[8] = {raw_h, pulse_scale, phase, image_h, image_scale, dphi, loss, stream};
+    const void* key[9] = {raw_h, pulse_scale, phase, image_h, image_scale, dphi, loss, stream,
+                          s->rc_fp32 ? (const void*)s->rc32 : (const void*)s->rc};
     bool same = s->graph != nullptr;
-    for (int i = 0; i < 8 && same; ++i) same = (key[i] == s->g_key[i]);
+    for (int i = 0; i < 9 && same; ++i) same = (key[i] == s->g_key[i]);
     if (!same) {
         if (s->graph) cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
@@ -817,7 +880,7 @@ extern "C" int mfft_sar_step_graph(mfft_sar* s, const void* raw_h, const float* 
             s->graph = nullptr;
             return cuda_error(e, "SAR graph capture");
         }
-        for (int i = 0; i < 8; ++i) s->g_key[i] = key[i];
+        for (int i = 0; i < 9; ++i) s->g_key[i] = key[i];
     }
     cudaError_t e = cudaGraphLaunch(s->graph, st);
     if (e != cudaSuccess) return cuda_error(e, "SAR graph launch");

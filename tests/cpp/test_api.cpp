@@ -26,6 +26,9 @@ int main() {
         for (auto v : y) EXPECT(std::abs(v - cfloat(1.f, 0.f)) < 1e-5f);
         auto z = f.inverse(y);
         EXPECT(std::abs(z[0] - cfloat(1.f, 0.f)) < 1e-5f && std::abs(z[1]) < 1e-5f);
+        // adjoint of the forward: F^H (all ones) = n * impulse
+        auto g = f.backward(y, MFFT_FORWARD);
+        EXPECT(std::abs(g[0] - cfloat((float)n, 0.f)) < 1e-5f * (float)n && std::abs(g[1]) < 1e-5f * (float)n);
     }
     {
         MetalFFT f(512);
