@@ -70,7 +70,7 @@ BYTES_PER_TRANSFORM = N * 8 * 2  # read + write, complex64
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=BATCH)
@@ -101,8 +101,67 @@ def traffic_per_launch(kernel):
     return v.get("bytes_per_launch") if isinstance(v, dict) else None
 
 
+class NvmlSampler:
+    """SM clock and clock-event reasons read through NVML every ~0.5 ms by a
+    host thread, started right before the timed region's first launch and
+    stopped after its final synchronize, so that a timed region of a few
+    milliseconds still gets samples taken while it runs (nvidia-smi samples
+    every 200 ms at best)."""
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, uuid):
+        self.samples = []
+        self.handle = None
+        self._stop = False
+        self._thread = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            u = str(uuid) if uuid else None
+            if u:
+                self.handle = pynvml.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM) if self.handle else None
+        except Exception:
+            self.handle = None
+            self.max_mhz = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop:
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                self.samples.append((mhz, rs))
+            except Exception:
+                return
+            time.sleep(0.0005)
+
+    def __enter__(self):
+        import threading
+        if self.handle is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop = True
+        if self._thread:
+            self._thread.join(timeout=2)
+
+    def summary(self):
+        if not self.samples:
+            return None
+        mhz = [m for m, _ in self.samples]
+        reasons = sorted({name for _, r in self.samples for bit, name in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(mhz), "sm_mhz_min": min(mhz), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(mhz), "source": "NVML, every ~0.5 ms inside the timed region"}
+
+
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms, plus the
+    NVML sampler over the timed region itself (summary() prefers it)."""
     FIELDS = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -111,6 +170,11 @@ class ClockSampler:
         self.uuid = uuid
         self.proc = None
         self.path = None
+        self.fast = NvmlSampler(uuid)
+
+    def region(self):
+        """Context manager around the timed region itself."""
+        return self.fast
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -149,14 +213,23 @@ class ClockSampler:
                 os.unlink(self.path)
             except OSError:
                 pass
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+        fast = self.fast.summary()
+        smi = None
+        if rows:
+            sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+            mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i] == "Active"})
+            smi = {"sm_mhz": statistics.median(sm) if sm else None,
+                   "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+        if fast:
+            if smi:
+                fast["nvidia_smi"] = smi
+                fast["reasons"] = sorted(set(fast["reasons"]) | set(smi["reasons"]))
+                if fast["sm_max_mhz"] is None:
+                    fast["sm_max_mhz"] = smi["sm_max_mhz"]
+            return fast
+        return smi or {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
 
 
 def make_input(batch, rank):
@@ -215,12 +288,20 @@ def link_ceiling(hin, hout, din, dout, transforms, reps=3):
             "link_note": "plain pinned copies of the same bytes, both directions at once"}
 
 
-def cpu_baseline(seconds=12.0):
+def tc4096_config(batch):
+    """The config of the default workload, the same in both arms."""
+    return {"workload": "batched C2C FFT N=4096 x %d lines per GPU, complex64, re/im N(0,1) seeded, forward"
+                        % batch,
+            "n": N, "batch_per_gpu": batch, "parallelism": "replicas",
+            "l2": "inputs larger than L2 (%d MiB read + %d MiB written per step)" % (batch // 32, batch // 32)}
+
+
+def cpu_baseline(batch, seconds=10.0):
     """The reference algorithm (FP32 radix-4 Stockham, oracle/) on all host
-    cores over a bounded sample of the same workload."""
+    cores over whole steps of the same workload (the full batch per step),
+    repeated for about `seconds`."""
     from oracle import oracle as O
-    sample = 1024
-    x = O.normal_c64((sample, N), seed=SEED)
+    x = make_input(batch, 0)
     O.ref_fft(x[:64])  # warm
     reps, t0 = 0, time.perf_counter()
     while True:
@@ -229,10 +310,33 @@ def cpu_baseline(seconds=12.0):
         if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
-    return {"value": reps * sample / dt, "unit": "transforms/s", "cores": O.max_threads(),
+    return {"value": reps * batch / dt, "unit": "transforms/s", "cores": O.max_threads(),
             "kind": "port",
-            "sample": "%d x %d lines of N=%d (of the 16384-line step), FP32 radix-4 Stockham "
-                      "restatement of the reference, OpenMP over lines" % (reps, sample, N)}
+            "sample": "%d whole steps of %d lines of N=%d in %.1f s, FP32 radix-4 Stockham restatement of the "
+                      "reference, OpenMP over lines" % (reps, batch, N, dt)}
+
+
+def cpu_scipy(batch, seconds=5.0):
+    """A second, third-party CPU point (not the reference's path, not an
+    oracle): scipy.fft (pocketfft) over the same steps, complex64, all host
+    threads."""
+    try:
+        import scipy.fft as sf
+    except Exception as e:  # pragma: no cover
+        return {"unavailable": str(e)}
+    x = make_input(batch, 0)
+    workers = os.cpu_count() or 1
+    sf.fft(x[:64], axis=-1, workers=workers)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        sf.fft(x, axis=-1, workers=workers)
+        reps += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": reps * batch / dt, "unit": "transforms/s", "cores": workers, "kind": "scipy.fft",
+            "sample": "%d whole steps of %d lines in %.1f s, scipy.fft.fft complex64, workers=%d (a labelled "
+                      "comparator: the reference's own CPU path is vDSP)" % (reps, batch, dt, workers)}
 
 
 def cpu_baseline_other(workload, seconds=8.0):
@@ -325,18 +429,26 @@ def cpu_baseline_other(workload, seconds=8.0):
 
 
 def run_reference(args, rank, world):
+    """The reference's CPU path for this workload (its FP32 radix-4 Stockham
+    restated in oracle/, all host cores): every step transforms the whole
+    16384-line batch of the GPU arm's config, so both arms time the same work."""
     if rank != 0:
         return
+    if args.workload != "tc4096":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the default workload only; "
+                                                              "every other workload's line carries its own "
+                                                              "cpu_baseline"}), flush=True)
+        return
     from oracle import oracle as O
-    sample = 512
-    x = O.normal_c64((sample, N), seed=SEED)
+    B = args.batch
+    x = make_input(B, 0)
     for _ in range(args.warmup):
         O.ref_fft(x)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         O.ref_fft(x)
     dt = time.perf_counter() - t0
-    v = args.steps * sample / dt
+    v = args.steps * B / dt
     cores = O.max_threads()
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "transforms/s",
@@ -344,12 +456,11 @@ def run_reference(args, rank, world):
         "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "gflop_per_s": v * fft_flops(N) / 1e9, "gflop_note": "5 N log2 N per transform",
-        "config": {"workload": "batched C2C FFT N=4096, complex64 N(0,1) seeded; each step a "
-                               "bounded sample of %d of the 16384 lines" % sample,
-                   "n": N, "batch": sample},
+        "config": tc4096_config(B),
+        "variant": "FP32 radix-4 Stockham (the reference's algorithm, host cores)",
         "cpu_baseline": {"value": v, "unit": "transforms/s", "cores": cores, "kind": "port",
-                         "sample": "%d lines of N=%d per step, FP32 radix-4 Stockham restatement "
-                                   "of the reference, OpenMP over lines" % (sample, N)},
+                         "sample": "%d whole steps of %d lines of N=%d in %.2f s, FP32 radix-4 Stockham "
+                                   "restatement of the reference, OpenMP over lines" % (args.steps, B, N, dt)},
         "e2e": {"value": v, "unit": "transforms/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -367,11 +478,12 @@ def timed(fn, steps, warmup, barrier, dist, uuid):
     e1 = torch.cuda.Event(enable_timing=True)
     stream = torch.cuda.current_stream()
     with ClockSampler(uuid) as clk:
-        e0.record(stream)
-        for i in range(steps):
-            fn(i)
-        e1.record(stream)
-        torch.cuda.synchronize()
+        with clk.region():
+            e0.record(stream)
+            for i in range(steps):
+                fn(i)
+            e1.record(stream)
+            torch.cuda.synchronize()
     barrier()
     ms = e0.elapsed_time(e1)
     from metalfft_b200 import dist as D
@@ -721,11 +833,12 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         with ClockSampler(uuid) as clk:
-            e0.record(stream)
-            for _ in range(args.steps):
-                f.exec(x, y, B, M.FORWARD, tc)
-            e1.record(stream)
-            torch.cuda.synchronize()
+            with clk.region():
+                e0.record(stream)
+                for _ in range(args.steps):
+                    f.exec(x, y, B, M.FORWARD, tc)
+                e1.record(stream)
+                torch.cuda.synchronize()
         barrier()
         ms = e0.elapsed_time(e1)
         ms_max = D.max_over_ranks(ms, device="cuda")
@@ -769,10 +882,33 @@ def main():
     dt = D.max_over_ranks(time.perf_counter() - t0, device="cuda")
     e2e = {"value": B * world * args.e2e_steps / dt, "unit": "transforms/s",
            "h2d_bytes_per_step": B * N * 8, "d2h_bytes_per_step": B * N * 8,
-           "steps": args.e2e_steps}
+           "steps": args.e2e_steps, "host_memory": "pinned"}
     e2e.update(link_ceiling(hin, hout, x, y, B * world))
+    # the same call on pageable host memory (what a Swift array is)
+    hin, hout = None, None
+    pin, pout = host, np.empty_like(host)
+
+    def e2e_pageable():
+        if tc:
+            st = M.lib.mfft_exec_c2c_tc(f._plan, ctypes.c_void_p(pin.ctypes.data), ctypes.c_void_p(pout.ctypes.data),
+                                        B, M.FORWARD, tc, M.HOST, None)
+        else:
+            st = M.lib.mfft_exec_c2c(f._plan, ctypes.c_void_p(pin.ctypes.data), ctypes.c_void_p(pout.ctypes.data),
+                                     B, M.FORWARD, M.HOST, None)
+        M._check(st)
+
+    e2e_pageable()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_pageable()
+    barrier()
+    dtp = D.max_over_ranks(time.perf_counter() - t0, device="cuda")
+    e2e["pageable"] = {"value": B * world * args.e2e_steps / dtp, "unit": "transforms/s",
+                       "steps": args.e2e_steps, "host_memory": "pageable (numpy), same call"}
 
     kernel_name = "k_fft_batched" if best == "fp32" else "k_fft4096_tcq"
+    config = tc4096_config(B)
     line = {
         "metric": METRIC,
         "value": r["transforms_per_s"],
@@ -786,10 +922,8 @@ def main():
         "vs_baseline": None,
         "dtype": "fp32" if best == "fp32" else ("fp16x3->fp32" if best == "tc_fp16_split3" else "bf16->fp32"),
         "data": "synthetic",
-        "config": {"workload": "batched C2C FFT N=4096 x %d lines per GPU, complex64, re/im "
-                               "N(0,1) seeded, forward" % B,
-                   "n": N, "batch_per_gpu": B, "variant": best, "parallelism": "replicas",
-                   "l2": "inputs larger than L2 (%d MiB read + %d MiB written per step)" % (B // 32, B // 32)},
+        "config": config,
+        "variant": best,
         "rel_rms": r["rel_rms"],
         "gflop_per_s": r["gflop_per_s"],
         "gflop_note": "5 N log2 N per transform",
@@ -803,7 +937,8 @@ def main():
         "e2e": e2e,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline()
+        line["cpu_baseline"] = cpu_baseline(B)
+        line["cpu_scipy"] = cpu_scipy(B)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -162,11 +162,23 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, ConvGeom<FFT>::MINB_FW
 }
 
 // backward: dx[0, nx) and per-walker partial dh spectra part[unit][FFT].
+// Blocks b, b+1 travel together, like the forward kernel's pairs:
+//   Z = FFT(g_b + i g_{b+1})   (windows of FFT samples of g from b*hop)
+//   W = FFT(x_b + i x_{b+1})   (hop samples of x each, zero-padded)
+//   dx_b + i dx_{b+1} = IFFT(Z conj H) on [0, hop)   (h real: both halves real)
+//   P += Z conj(W)
+// With G_b, X_b the Hermitian parts of Z and W, G_b conj X_b + G_{b+1} conj
+// X_{b+1} = (P_k + conj P_{-k}) / 2, so the symmetrisation is done once, on
+// the summed spectrum (k_dh_finish), and no block needs a Hermitian split.
+// Z waits in shared memory (or in this walker's global stash row `zs` when
+// shared memory is full) while W is transformed: one 16-value array is live
+// at a time.  dx == nullptr skips the dx transform.
 template <int FFT>
 __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
     k_conv_bwd(const float* __restrict__ x, long long nx, const float* __restrict__ g, long long ny,
                const float2* __restrict__ H, const float2* __restrict__ tw, int hop, long long nblocks,
-               long long blocks_per_unit, float* __restrict__ dx, float2* __restrict__ part) {
+               long long blocks_per_unit, float* __restrict__ dx, float2* __restrict__ part,
+               float2* __restrict__ zs) {
     // the dh spectrum accumulates in shared memory, or directly in this
     // walker's row of `part` when shared memory is too small
     using G = ConvGeom<FFT>;
@@ -182,72 +194,65 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
     const long long mine = b1 > b0 ? b1 - b0 : 0;
     const float sc = 1.0f / (float)FFT;
 
-    // dh spectrum accumulator: bin k lives at D[k], owned by one thread
+    // P accumulator and Z stash: bin k at D[k] / Zs[k], owned by one thread
     float2* D = G::ACC_SMEM ? smem + G::SMEM_F2 + lf * FFT : part + unit * FFT;
-    // this thread's slots of the stash (same bins as D)
-    float2* stash = smem + G::SMEM_F2 + G::LINES * FFT + lf * FFT;
+    float2* Zs = G::STASH ? smem + G::SMEM_F2 + G::LINES * FFT + lf * FFT : zs + unit * FFT;
 #pragma unroll
     for (int m = 0; m < CONV_E; ++m) D[t + m * T] = make_float2(0.f, 0.f);
 
     for (long long it = 0; it < blocks_per_unit; it += 2) {
-        // S holds block 0's dx spectrum, then conj(S0 + i S1) for the shared inverse
-        float2 S[CONV_E];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const long long b = b0 + it + q;
-            const bool active = (it + q) < mine;
-            const long long base = b * hop;
-            const int glim = active ? clamp_count(ny - base, FFT) : 0;
-            const int xlim = active ? clamp_count(nx - base, hop) : 0;
-            const float* gb = g + base;
-            const float* xb = x + base;
-            float2 v[CONV_E];
+        const long long base0 = (b0 + it) * hop, base1 = base0 + hop;
+        const bool a0 = it < mine, a1 = it + 1 < mine;
+        float2 v[CONV_E];
+        {
+            const int l0 = a0 ? clamp_count(ny - base0, FFT) : 0;
+            const int l1 = a1 ? clamp_count(ny - base1, FFT) : 0;
+            const float* g0 = g + base0;
+            const float* g1 = g + base1;
 #pragma unroll
             for (int m = 0; m < CONV_E; ++m) {
                 const int i = t + m * T;
-                float re = 0.f, im = 0.f;
-                if (i < glim) re = __ldcs(gb + i);
-                if (i < xlim) im = __ldcs(xb + i);
-                v[m] = make_float2(re, im);
+                v[m] = make_float2(i < l0 ? __ldcs(g0 + i) : 0.f, i < l1 ? __ldcs(g1 + i) : 0.f);
             }
-            fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
-            // Hermitian split needs Z[(FFT - k) mod FFT]: exchange through smem
+        }
+        fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
 #pragma unroll
-            for (int m = 0; m < CONV_E; ++m) buf[t + m * T] = v[m];
-            line_sync<G::WS>();
+        for (int m = 0; m < CONV_E; ++m) Zs[t + m * T] = v[m];
+        {
+            const int l0 = a0 ? clamp_count(nx - base0, hop) : 0;
+            const int l1 = a1 ? clamp_count(nx - base1, hop) : 0;
+            const float* x0 = x + base0;
+            const float* x1 = x + base1;
+#pragma unroll
+            for (int m = 0; m < CONV_E; ++m) {
+                const int i = t + m * T;
+                v[m] = make_float2(i < l0 ? __ldcs(x0 + i) : 0.f, i < l1 ? __ldcs(x1 + i) : 0.f);
+            }
+        }
+        fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
+#pragma unroll
+        for (int m = 0; m < CONV_E; ++m) {
+            const int k = t + m * T;
+            D[k] = cadd(D[k], cmul(Zs[k], cconj(v[m])));
+        }
+        if (dx) {
+            // conj(Z conj H): the inverse as a forward transform of the conjugate
 #pragma unroll
             for (int m = 0; m < CONV_E; ++m) {
                 const int k = t + m * T;
-                const float2 zc = cconj(buf[(FFT - k) & (FFT - 1)]);
-                // Gk = (Z + conj Zr)/2, Xk = (Z - conj Zr)/(2i)
-                const float2 Gk = make_float2(0.5f * (v[m].x + zc.x), 0.5f * (v[m].y + zc.y));
-                const float2 dZ = make_float2(0.5f * (v[m].x - zc.x), 0.5f * (v[m].y - zc.y));
-                const float2 Xk = make_float2(dZ.y, -dZ.x);
-                const float2 Sk = cmul(Gk, cconj(__ldg(H + k)));
-                D[k] = cadd(D[k], cmul(Gk, cconj(Xk)));
-                if (q == 0) {
-                    if constexpr (G::STASH) stash[k] = Sk;
-                    else S[m] = Sk;
-                } else {
-                    const float2 S0 = G::STASH ? stash[k] : S[m];
-                    S[m] = cconj(make_float2(S0.x - Sk.y, S0.y + Sk.x));
-                }
+                v[m] = cconj(cmul(Zs[k], cconj(__ldg(H + k))));
             }
-            line_sync<G::WS>();
-        }
-        // one inverse for both blocks: IFFT(S0 + i S1) = s0 + i s1 (both real)
-        fft_regs<FFT, CONV_E, G::WS>(S, t, buf, tw);
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const long long base = (b0 + it + q) * hop;
-            const int lim = (it + q) < mine ? clamp_count(nx - base, hop) : 0;
-            float* db = dx + base;
+            fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
+            const int l0 = a0 ? clamp_count(nx - base0, hop) : 0;
+            const int l1 = a1 ? clamp_count(nx - base1, hop) : 0;
+            float* d0 = dx + base0;
+            float* d1 = dx + base1;
 #pragma unroll
             for (int m = 0; m < CONV_E; ++m) {
                 const int i = t + m * T;
-                // r = conj(S)/FFT: re = block b, im = block b+1
-                const float val = (q == 0 ? S[m].x : -S[m].y) * sc;
-                if (i < lim) __stcs(db + i, val);
+                // IFFT = conj(FFT(conj)) / FFT: re = block b, im = block b+1
+                if (i < l0) __stcs(d0 + i, v[m].x * sc);
+                if (i < l1) __stcs(d1 + i, -v[m].y * sc);
             }
         }
     }
@@ -279,7 +284,8 @@ __global__ void __launch_bounds__(SUM_BINS * SUM_RUNS)
     out[k] = tot;
 }
 
-// dh[k] = Re IFFT(D)[k], k < K (one line)
+// dh[k] = Re IFFT(S)[k], k < K (one line), S_k = (P_k + conj P_{-k}) / 2 the
+// Hermitian part of the summed pair spectra P (k_conv_bwd)
 template <int FFT>
 __global__ void __launch_bounds__(ConvGeom<FFT>::T) k_dh_finish(const float2* __restrict__ D, const float2* __restrict__ tw,
                                                                 int K, float* __restrict__ dh) {
@@ -288,7 +294,11 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::T) k_dh_finish(const float2* __
     const int t = threadIdx.x;
     float2 v[CONV_E];
 #pragma unroll
-    for (int m = 0; m < CONV_E; ++m) v[m] = cconj(D[t + m * T]);
+    for (int m = 0; m < CONV_E; ++m) {
+        const int k = t + m * T;
+        const float2 a = D[k], b = D[(FFT - k) & (FFT - 1)];
+        v[m] = cconj(make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y)));
+    }
     fft_regs<FFT, CONV_E, (T <= 32)>(v, t, PadLine{smem}, tw);
 #pragma unroll
     for (int m = 0; m < CONV_E; ++m) {
@@ -359,10 +369,11 @@ struct LineKernels {
     int threads, lines, smem, line_smem;
     cudaError_t (*prepare)();
     bool acc_smem;
+    bool stash_smem;  // backward: Z stash in shared memory (else a global row per walker)
     void (*fwd)(dim3, int, cudaStream_t, const float*, long long, float*, long long, const float2*, const float2*, int,
                 long long, long long, int, float*);
     void (*bwd)(dim3, int, cudaStream_t, const float*, long long, const float*, long long, const float2*,
-                const float2*, int, long long, long long, float*, float2*);
+                const float2*, int, long long, long long, float*, float2*, float2*);
     void (*dh)(cudaStream_t, const float2*, const float2*, int, float*);
     void (*corr)(cudaStream_t, const float*, long long, const float*, long long, const float2*, float*);
     void (*analyze)(cudaStream_t, const float*, const float*, const float2*, float2*);
@@ -387,9 +398,10 @@ void l_fwd(dim3 grid, int smem, cudaStream_t s, const float* x, long long nx, fl
 }
 template <int FFT>
 void l_bwd(dim3 grid, int, cudaStream_t s, const float* x, long long nx, const float* g, long long ny,
-           const float2* H, const float2* tw, int hop, long long nblocks, long long bpu, float* dx, float2* part) {
+           const float2* H, const float2* tw, int hop, long long nblocks, long long bpu, float* dx, float2* part,
+           float2* zs) {
     k_conv_bwd<FFT><<<grid, ConvGeom<FFT>::THREADS, ConvGeom<FFT>::SMEM_BYTES_BWD, s>>>(x, nx, g, ny, H, tw, hop,
-                                                                                     nblocks, bpu, dx, part);
+                                                                                     nblocks, bpu, dx, part, zs);
 }
 template <int FFT>
 void l_dh(cudaStream_t s, const float2* D, const float2* tw, int K, float* dh) {
@@ -406,7 +418,8 @@ void l_an(cudaStream_t s, const float* smp, const float* w, const float2* tw, fl
 
 #define MFFT_LINEK(F)                                                                                       \
     {F,           ConvGeom<F>::THREADS, ConvGeom<F>::LINES, ConvGeom<F>::SMEM_BYTES, spad_size(F) * 8,     \
-     &prep_line<F>, ConvGeom<F>::ACC_SMEM, &l_fwd<F>, &l_bwd<F>, &l_dh<F>, &l_corr<F>, &l_an<F>}
+     &prep_line<F>, ConvGeom<F>::ACC_SMEM, ConvGeom<F>::STASH, &l_fwd<F>, &l_bwd<F>, &l_dh<F>, &l_corr<F>,     \
+     &l_an<F>}
 
 const LineKernels g_linek[] = {MFFT_LINEK(64),   MFFT_LINEK(128),  MFFT_LINEK(256),
                                MFFT_LINEK(512),  MFFT_LINEK(1024), MFFT_LINEK(2048),
@@ -607,18 +620,20 @@ static int conv_bwd_device(mfft_conv* c, const float* x, long long nx, const flo
     units = nblocks > 0 ? (nblocks + bpu - 1) / bpu : 1;
     const long long ctas = (units + c->lk->lines - 1) / c->lk->lines;
     const long long slots = ctas * c->lk->lines;
-    if (slots > c->part_units) {
+    // rows of partial spectra, then (when shared memory cannot hold it) one
+    // Z stash row per walker
+    const long long rows = c->lk->stash_smem ? slots : 2 * slots;
+    if (rows > c->part_units) {
         if (c->part) cudaFree(c->part);
         c->part = nullptr;
         c->part_units = 0;
-        cudaError_t e = cudaMalloc(&c->part, sizeof(float2) * c->fft * slots);
+        cudaError_t e = cudaMalloc(&c->part, sizeof(float2) * c->fft * rows);
         if (e != cudaSuccess) return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "dh partials: %s", cudaGetErrorString(e));
-        c->part_units = slots;
+        c->part_units = rows;
     }
-    float* dxp = dx;
-    if (!dxp) dxp = nullptr;
-    c->lk->bwd(dim3((unsigned)ctas), c->lk->smem, s, x, nx, gy, ny, c->H, c->tw, (int)c->hop, nblocks, bpu,
-               dx ? dx : reinterpret_cast<float*>(c->part) /* unused when nblocks==0 */, c->part);
+    float2* zs = c->lk->stash_smem ? nullptr : c->part + slots * c->fft;
+    c->lk->bwd(dim3((unsigned)ctas), c->lk->smem, s, x, nx, gy, ny, c->H, c->tw, (int)c->hop, nblocks, bpu, dx,
+               c->part, zs);
     if (dh) {
         k_sum_spectra<<<(unsigned)(c->fft / SUM_BINS), SUM_BINS * SUM_RUNS, 0, s>>>(c->part, slots, (int)c->fft,
                                                                                  c->Dsum);

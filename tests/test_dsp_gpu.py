@@ -162,6 +162,55 @@ def test_autocorrelation_peak_is_energy(M):
     assert int(np.argmax(r)) == 0
 
 
+# ---- golden fixtures (tests/golden/make_golden.py: the reference's host loops
+# ---- transliterated to numpy over FP64 pocketfft, independent of oracle/)
+
+def _golden(name):
+    import os
+    return np.load(os.path.join(os.path.dirname(__file__), "golden", name))
+
+
+def test_golden_convolver_cases(M):
+    """Convolver.apply and its adjoint on the reference's edge cases: an empty
+    signal, shorter than one hop, K = 1, ending on a hop boundary, hop 2."""
+    z = _golden("conv_golden.npz")
+    for name in z["cases"]:
+        x, h, y, t = z[name + "_x"], z[name + "_h"], z[name + "_y"], z[name + "_t"]
+        conv = M.Convolver(h, int(z[name + "_fft"]))
+        yg = conv.apply(x)
+        assert yg.shape == y.shape, name
+        if len(x) == 0:
+            assert not yg.any()
+            continue
+        assert rel(yg, y) < 2e-6, (name, rel(yg, y))
+        g = (y - t).astype(np.float32)
+        dx, dh = conv.backward(x, g)
+        rdx, rdh = O.conv_adjoint64(x, h, g)  # at the FP32 gradient the GPU saw
+        assert rel(dx, rdx) < 1e-5 and rel(dh, rdh) < 1e-5, name
+        assert rel(dx, z[name + "_dx"]) < 1e-5 and rel(dh, z[name + "_dh"]) < 1e-5, name
+
+
+def test_golden_correlator_cases(M):
+    z = _golden("corr_golden.npz")
+    for name in z["cases"]:
+        a, b, r = z[name + "_a"], z[name + "_b"], z[name + "_r"]
+        out = M.Correlator(int(z[name + "_fft"])).cross(a, b)
+        assert out.shape == r.shape, name
+        scale = max(np.max(np.abs(r)), float(np.sum(a.astype(np.float64) ** 2)))
+        assert np.max(np.abs(out - r)) <= 2e-6 * scale, name
+
+
+def test_golden_analyzer_windows(M):
+    z = _golden("analyzer_golden.npz")
+    n = len(z["w_rect"])
+    s = z["samples"]
+    for key, wt in [("flattop", M.WindowType(M.WindowType.FLAT_TOP)), ("kaiser6", M.WindowType.kaiser(6.0)),
+                    ("kaiser9", M.WindowType.kaiser(9.5)), ("rect", M.WindowType(M.WindowType.RECTANGULAR))]:
+        an = M.FFTAnalyzer(n, 48000.0, wt)
+        assert O.rel_rms(an.analyze(s[:n]).complex[None], z["X0_" + key][None]) < 2e-6, key
+        assert O.rel_rms(an.analyze(s, offset=n + 17).complex[None], z["X1_" + key][None]) < 2e-6, key
+
+
 # ---- FFTAnalyzer -----------------------------------------------------------
 
 @pytest.mark.parametrize("kind", [0, 1, 2, 3, 5])

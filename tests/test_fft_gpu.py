@@ -91,8 +91,9 @@ def test_golden_fixtures(M):
     import os
     z = np.load(os.path.join(os.path.dirname(__file__), "golden", "fft_golden.npz"))
     for n in [64, 512, 4096]:
-        y = M.MetalFFT(n).forward_batch(z["x_%d" % n])
-        assert O.rel_rms(y, z["X_%d" % n]) < TOL
+        f = M.MetalFFT(n)
+        assert O.rel_rms(f.forward_batch(z["x_%d" % n]), z["X_%d" % n]) < TOL
+        assert O.rel_rms(f.inverse_batch(z["x_%d" % n]), z["Xi_%d" % n]) < TOL
 
 
 def test_forward_into_and_multichannel(M):

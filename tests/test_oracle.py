@@ -187,16 +187,77 @@ def test_ct_dif_variant_agrees_with_oracle():
 
 # ---- golden fixtures --------------------------------------------------------
 
+def _golden(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
 def test_golden_fft_fixtures():
-    z = np.load(os.path.join(GOLDEN, "fft_golden.npz"))
-    for key in z.files:
-        if not key.startswith("x_"):
+    # fixtures from pocketfft (tests/golden/make_golden.py), not from the oracle
+    z = _golden("fft_golden.npz")
+    for n in [64, 512, 4096]:
+        x, X, Xi = z["x_%d" % n], z["X_%d" % n], z["Xi_%d" % n]
+        assert l2(O.truth(x), X) < 1e-13
+        assert l2(O.truth(x, inverse=True), Xi) < 1e-13
+        assert l2(O.fft64(x), X) < 1e-13
+        assert O.rel_rms(O.ref_fft(x), X) < 1e-6          # the FP32 restatement
+        assert O.rel_rms(O.ref_fft(x, inverse=True), Xi) < 1e-6
+
+
+def test_golden_convolver_fixtures():
+    """The oracle's FP64 overlap-add, its FP32 restatement of the reference's
+    loop and its analytic adjoint against the transliterated reference loop
+    (Convolve.swift:36-76) on the reference's edge cases: an empty signal, a
+    signal shorter than one hop, K = 1, a signal ending on a hop boundary,
+    hop 2."""
+    z = _golden("conv_golden.npz")
+    for name in z["cases"]:
+        x, h, y, t = z[name + "_x"], z[name + "_h"], z[name + "_y"], z[name + "_t"]
+        fft = int(z[name + "_fft"])
+        assert y.shape == (len(x) + len(h) - 1,)
+        y64 = O.conv64(x, h, fft)
+        assert y64.shape == y.shape, name
+        scale = max(np.max(np.abs(y)), 1e-30)
+        assert np.max(np.abs(y64 - y)) <= 1e-12 * scale, name
+        y32 = O.ref_conv(x, h, fft)
+        assert y32.shape == y.shape, name
+        assert np.max(np.abs(y32 - y)) <= 2e-6 * scale, name
+        if len(x) == 0:
+            assert not y64.any() and not y32.any()
             continue
-        n = int(key[2:])
-        x = z[key]
-        assert O.rel_rms(O.ref_fft(x), z["X_%d" % n]) < 1e-5
-        assert l2(O.truth(x), z["X_%d" % n]) < 1e-13
-        assert l2(O.truth(z["X_%d" % n].astype(np.complex64), inverse=True), x) < 1e-6
+        dx, dh = O.conv_adjoint64(x, h, (y - t))
+        assert np.max(np.abs(dx - z[name + "_dx"])) <= 1e-11 * np.max(np.abs(z[name + "_dx"])), name
+        assert np.max(np.abs(dh - z[name + "_dh"])) <= 1e-11 * np.max(np.abs(z[name + "_dh"])), name
+
+
+def test_golden_correlator_fixtures():
+    """corr64 / ref_corr against the transliterated Correlator.cross
+    (Correlate.swift:27-61): zero padding, truncation of inputs longer than
+    fftSize, an empty input, and auto()."""
+    z = _golden("corr_golden.npz")
+    for name in z["cases"]:
+        a, b, r = z[name + "_a"], z[name + "_b"], z[name + "_r"]
+        fft = int(z[name + "_fft"])
+        scale = max(np.max(np.abs(r)), 1e-30)
+        assert np.max(np.abs(O.corr64(a, b, fft) - r)) <= 1e-12 * scale, name
+        assert np.max(np.abs(O.ref_corr(a, b, fft) - r)) <= 2e-6 * max(scale, np.sum(a * a)), name
+
+
+def test_golden_window_and_analyzer_fixtures():
+    """The flat-top and Kaiser coefficients and FFTAnalyzer.analyze (window x
+    samples in FP32, FFT) against the transliterated reference
+    (Window.swift:51-75,100-110, FFTAnalyzer.swift:93-116)."""
+    z = _golden("analyzer_golden.npz")
+    n = len(z["w_rect"])
+    assert np.max(np.abs(O.window(3, n) - z["w_flattop"])) < 1e-6
+    assert np.max(np.abs(O.window(4, n, 6.0) - z["w_kaiser6"])) < 1e-9
+    assert np.max(np.abs(O.window(4, n, 9.5) - z["w_kaiser9"])) < 1e-9
+    assert np.all(O.window(5, n) == 1.0)
+    s = z["samples"]
+    for key, kind, beta in [("flattop", 3, 6.0), ("kaiser6", 4, 6.0), ("kaiser9", 4, 9.5), ("rect", 5, 6.0)]:
+        w = np.asarray(O.window(kind, n, beta), np.float32)
+        for tag, off in [("X0_", 0), ("X1_", n + 17)]:
+            win = (s[off:off + n] * w).astype(np.float32)
+            assert l2(O.fft64(win.astype(np.complex128)[None])[0], z[tag + key]) < 1e-6, (key, tag)
 
 
 # ---- convolver / correlator --------------------------------------------------
