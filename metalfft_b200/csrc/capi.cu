@@ -10,10 +10,13 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <condition_variable>
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <utility>
+#include <vector>
 
 #include "capi_internal.h"
 #include "tma.cuh"
@@ -195,6 +198,8 @@ extern "C" int mfft_context_destroy(mfft_ctx* ctx) {
         }
         cudaFree(ctx->stage);
     }
+    if (ctx->hstage) cudaFreeHost(ctx->hstage);
+    mfft::host_copier_free(ctx->copier);
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     for (auto& kv : ctx->twiddles) cudaFree(kv.second);
     cudaFree(ctx->dev_err);
@@ -412,6 +417,99 @@ int run_host_staged(mfft_ctx* ctx, const void* in, void* out, size_t in_bytes, s
     return st;
 }
 
+// Parallel memcpy on a fixed pool of host threads: copy() splits a copy into
+// one part per worker (and one for the caller) and returns when all are done.
+struct HostCopier {
+    explicit HostCopier(int workers) {
+        for (int i = 0; i < workers; ++i) th_.emplace_back([this, i] { run(i); });
+    }
+    ~HostCopier() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : th_) t.join();
+    }
+    void copy(void* dst, const void* src, size_t bytes) {
+        const int parts = (int)th_.size() + 1;
+        if (bytes < ((size_t)1 << 20) || parts == 1) {
+            memcpy(dst, src, bytes);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            dst_ = (char*)dst;
+            src_ = (const char*)src;
+            bytes_ = bytes;
+            parts_ = parts;
+            pending_ = (int)th_.size();
+            ++gen_;
+        }
+        cv_.notify_all();
+        part(parts - 1);
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [this] { return pending_ == 0; });
+    }
+
+   private:
+    void part(int i) {
+        // 4 KiB-aligned split points
+        const size_t step = ((bytes_ / parts_) + 4095) & ~(size_t)4095;
+        const size_t a = step * (size_t)i, b = a + step < bytes_ ? a + step : bytes_;
+        if (a < b) memcpy(dst_ + a, src_ + a, b - a);
+    }
+    void run(int i) {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            part(i);
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_;
+    bool stop_ = false;
+    uint64_t gen_ = 0;
+    char* dst_ = nullptr;
+    const char* src_ = nullptr;
+    size_t bytes_ = 0;
+    int parts_ = 1, pending_ = 0;
+};
+
+void host_copier_free(HostCopier* c) { delete c; }
+
+// host memory the driver cannot DMA from directly (not page-locked)
+static bool pageable(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();  // (older drivers report unregistered memory as an error)
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+static int hstage_init(mfft_ctx* ctx) {
+    if (ctx->hstage) return MFFT_SUCCESS;
+    cudaError_t e = cudaHostAlloc(&ctx->hstage, STAGE_SLOT_BYTES * 2 * STAGE_SLOTS, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        ctx->hstage = nullptr;
+        return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "pinned host staging: %s", cudaGetErrorString(e));
+    }
+    if (!ctx->copier) {
+        const unsigned hw = std::thread::hardware_concurrency();
+        ctx->copier = new HostCopier((int)(hw >= 16 ? 7 : hw >= 4 ? hw / 2 - 1 : 0));
+    }
+    return MFFT_SUCCESS;
+}
+
 static int stage_init(mfft_ctx* ctx) {
     if (ctx->h2d) return MFFT_SUCCESS;
     cudaError_t e = cudaMalloc(&ctx->stage, STAGE_SLOT_BYTES * 2 * STAGE_SLOTS);
@@ -458,24 +556,52 @@ int run_host_lines(mfft_ctx* ctx, const void* in, void* out, int64_t lines, size
     std::lock_guard<std::mutex> lk(ctx->stage_mu);
     int st = stage_init(ctx);
     if (st) return st;
+    // Pageable host arrays (what a Swift or numpy array is) go through pinned
+    // host slots: the driver would otherwise stage each copy itself,
+    // synchronously and on one thread, and the chunks would not overlap.
+    const bool stage_host = pageable(in) || pageable(out);
+    if (stage_host) {
+        st = hstage_init(ctx);
+        if (st) return st;
+    }
     cudaStream_t sc = ctx->stream, sh = ctx->h2d, sd = ctx->d2h;
     char* slot = (char*)ctx->stage;
+    char* hslot = (char*)ctx->hstage;
     cudaError_t e = cudaSuccess;
     // uploads start after the compute stream's earlier work (the slots may
     // still be read by the previous call's last transforms)
     e = cudaEventRecord(ctx->ev_done[0], sc);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(sh, ctx->ev_done[0], 0);
     const int64_t nch = (lines + per - 1) / per;
+    // pageable output: chunk c's result leaves its pinned slot for the
+    // caller's array once its download is done
+    auto drain = [&](int64_t c) {
+        const int k = (int)(c % STAGE_SLOTS);
+        const int64_t l0 = c * per, nl = lines - l0 < per ? lines - l0 : per;
+        cudaError_t es = cudaEventSynchronize(ctx->ev_down[k]);
+        if (es != cudaSuccess) return es;
+        ctx->copier->copy((char*)out + (size_t)l0 * out_line, hslot + ((size_t)k * 2 + 1) * STAGE_SLOT_BYTES,
+                          (size_t)nl * out_line);
+        return cudaSuccess;
+    };
     for (int64_t c = 0; c < nch && e == cudaSuccess && !st; ++c) {
         const int k = (int)(c % STAGE_SLOTS);
         const int64_t l0 = c * per, nl = lines - l0 < per ? lines - l0 : per;
         char* din = slot + (size_t)k * 2 * STAGE_SLOT_BYTES;
         char* dout = in_place ? din : din + STAGE_SLOT_BYTES;
+        const char* src = (const char*)in + (size_t)l0 * in_line;
+        if (stage_host) {
+            // the pinned slots of chunk c - STAGE_SLOTS are free once its
+            // download is done and its result copied out
+            if (c >= STAGE_SLOTS) e = drain(c - STAGE_SLOTS);
+            if (e != cudaSuccess) break;
+            char* hin = hslot + (size_t)k * 2 * STAGE_SLOT_BYTES;
+            ctx->copier->copy(hin, src, (size_t)nl * in_line);
+            src = hin;
+        }
         // slot k is free once the download of chunk c - STAGE_SLOTS is done
         if (c >= STAGE_SLOTS) e = cudaStreamWaitEvent(sh, ctx->ev_down[k], 0);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(din, (const char*)in + (size_t)l0 * in_line, (size_t)nl * in_line,
-                                cudaMemcpyHostToDevice, sh);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(din, src, (size_t)nl * in_line, cudaMemcpyHostToDevice, sh);
         if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_up[k], sh);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(sc, ctx->ev_up[k], 0);
         if (e != cudaSuccess) break;
@@ -483,11 +609,12 @@ int run_host_lines(mfft_ctx* ctx, const void* in, void* out, int64_t lines, size
         if (st) break;
         e = cudaEventRecord(ctx->ev_done[k], sc);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(sd, ctx->ev_done[k], 0);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync((char*)out + (size_t)l0 * out_line, dout, (size_t)nl * out_line,
-                                cudaMemcpyDeviceToHost, sd);
+        char* dst = stage_host ? hslot + ((size_t)k * 2 + 1) * STAGE_SLOT_BYTES : (char*)out + (size_t)l0 * out_line;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dst, dout, (size_t)nl * out_line, cudaMemcpyDeviceToHost, sd);
         if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_down[k], sd);
     }
+    if (stage_host && !st && e == cudaSuccess)
+        for (int64_t c = nch > STAGE_SLOTS ? nch - STAGE_SLOTS : 0; c < nch && e == cudaSuccess; ++c) e = drain(c);
     if (!st && e != cudaSuccess) st = cuda_error(e, "staged copies");
     cudaError_t e1 = cudaStreamSynchronize(sh), e2 = cudaStreamSynchronize(sc), e3 = cudaStreamSynchronize(sd);
     if (!st && e1 != cudaSuccess) st = cuda_error(e1, "execution");

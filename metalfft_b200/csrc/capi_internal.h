@@ -11,6 +11,11 @@
 #include "../../include/mfft.h"
 #include "kernels.h"
 
+namespace mfft {
+struct HostCopier;
+void host_copier_free(HostCopier* c);
+}  // namespace mfft
+
 #define MFFT_MAX_N (1 << 20)
 #define MFFT_MAX_SINGLE_N 16384
 
@@ -32,6 +37,10 @@ struct mfft_ctx {
     cudaStream_t h2d = nullptr, d2h = nullptr;
     void* stage = nullptr;
     cudaEvent_t ev_up[4] = {}, ev_done[4] = {}, ev_down[4] = {};
+    // pageable host arrays: pinned host slots (in and out per staging slot)
+    // filled and drained by a small pool of host threads
+    void* hstage = nullptr;
+    mfft::HostCopier* copier = nullptr;
 };
 
 namespace mfft {

@@ -200,33 +200,35 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
 #pragma unroll
     for (int m = 0; m < CONV_E; ++m) D[t + m * T] = make_float2(0.f, 0.f);
 
-    for (long long it = 0; it < blocks_per_unit; it += 2) {
-        const long long base0 = (b0 + it) * hop, base1 = base0 + hop;
+    // this walker's span from one base pointer each, 32-bit offsets inside it
+    const long long ubase = b0 * hop;
+    const float* gu = g + ubase;
+    const float* xu = x + ubase;
+    float* du = dx ? dx + ubase : nullptr;
+    const long long ny_u = ny - ubase, nx_u = nx - ubase;
+    for (int it = 0; it < blocks_per_unit; it += 2) {
+        const int off0 = it * hop, off1 = off0 + hop;
         const bool a0 = it < mine, a1 = it + 1 < mine;
         float2 v[CONV_E];
         {
-            const int l0 = a0 ? clamp_count(ny - base0, FFT) : 0;
-            const int l1 = a1 ? clamp_count(ny - base1, FFT) : 0;
-            const float* g0 = g + base0;
-            const float* g1 = g + base1;
+            const int l0 = a0 ? clamp_count(ny_u - off0, FFT) : 0;
+            const int l1 = a1 ? clamp_count(ny_u - off1, FFT) : 0;
 #pragma unroll
             for (int m = 0; m < CONV_E; ++m) {
                 const int i = t + m * T;
-                v[m] = make_float2(i < l0 ? __ldcs(g0 + i) : 0.f, i < l1 ? __ldcs(g1 + i) : 0.f);
+                v[m] = make_float2(i < l0 ? __ldcs(gu + off0 + i) : 0.f, i < l1 ? __ldcs(gu + off1 + i) : 0.f);
             }
         }
         fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
 #pragma unroll
         for (int m = 0; m < CONV_E; ++m) Zs[t + m * T] = v[m];
         {
-            const int l0 = a0 ? clamp_count(nx - base0, hop) : 0;
-            const int l1 = a1 ? clamp_count(nx - base1, hop) : 0;
-            const float* x0 = x + base0;
-            const float* x1 = x + base1;
+            const int l0 = a0 ? clamp_count(nx_u - off0, hop) : 0;
+            const int l1 = a1 ? clamp_count(nx_u - off1, hop) : 0;
 #pragma unroll
             for (int m = 0; m < CONV_E; ++m) {
                 const int i = t + m * T;
-                v[m] = make_float2(i < l0 ? __ldcs(x0 + i) : 0.f, i < l1 ? __ldcs(x1 + i) : 0.f);
+                v[m] = make_float2(i < l0 ? __ldcs(xu + off0 + i) : 0.f, i < l1 ? __ldcs(xu + off1 + i) : 0.f);
             }
         }
         fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
             const int k = t + m * T;
             D[k] = cadd(D[k], cmul(Zs[k], cconj(v[m])));
         }
-        if (dx) {
+        if (du) {
             // conj(Z conj H): the inverse as a forward transform of the conjugate
 #pragma unroll
             for (int m = 0; m < CONV_E; ++m) {
@@ -243,16 +245,14 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
                 v[m] = cconj(cmul(Zs[k], cconj(__ldg(H + k))));
             }
             fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
-            const int l0 = a0 ? clamp_count(nx - base0, hop) : 0;
-            const int l1 = a1 ? clamp_count(nx - base1, hop) : 0;
-            float* d0 = dx + base0;
-            float* d1 = dx + base1;
+            const int l0 = a0 ? clamp_count(nx_u - off0, hop) : 0;
+            const int l1 = a1 ? clamp_count(nx_u - off1, hop) : 0;
 #pragma unroll
             for (int m = 0; m < CONV_E; ++m) {
                 const int i = t + m * T;
                 // IFFT = conj(FFT(conj)) / FFT: re = block b, im = block b+1
-                if (i < l0) __stcs(d0 + i, v[m].x * sc);
-                if (i < l1) __stcs(d1 + i, -v[m].y * sc);
+                if (i < l0) __stcs(du + off0 + i, v[m].x * sc);
+                if (i < l1) __stcs(du + off1 + i, -v[m].y * sc);
             }
         }
     }

@@ -13,8 +13,9 @@
 // Each product is D (128 x 64, FP32 in TMEM) = G (128 x 128) * B (128 x 64):
 // G is the realified DFT-64 matrix, row 2k+b = component b (re/im) of output
 // k, column 2n+a = component a of input n; B holds one line's data with the
-// same interleaved re/im index along K.  G is the A operand (K-major, loaded
-// into shared memory once per CTA); the line is the B operand: MN-major for
+// same interleaved re/im index along K.  G is the A operand, K-major, held in
+// tensor memory for the whole kernel (lane m = row m, two 16-bit K values per
+// 32-bit column); the line is the B operand in shared memory: MN-major for
 // stage 1 (straight from the input layout), K-major for stage 2 (written by
 // the stage-1 epilogue).
 //
@@ -26,14 +27,26 @@
 //               scales are undone exactly in the epilogues.
 //   BF16:       one product of bf16 operands.
 //
-// One CTA of 512 threads per SM holds G once and runs four independent
-// pipelines of 128 threads, one line each at a time (four lines in flight per
-// SM), each with its own B buffers, TMEM columns, commit mbarrier and named
-// barrier.  The stage-2 scale is s1/64 (a DFT-64 grows magnitudes by at most
-// 64), so no reduction sits between the two products.  A pipeline's first
-// thread issues its MMAs and waits on the commit mbarrier with a time limit;
-// a timeout sets the device error word and the pipeline leaves its loop; the
-// CTA then frees its TMEM and returns.
+// One persistent CTA per SM, warp-specialised, every hand-off an mbarrier:
+//   converter warps 0-3   load a line (streaming loads, the line two ahead
+//                         prefetched into L2), find its power-of-two scale,
+//                         write the stage-1 operand (hi/lo) into one of
+//                         three operand buffers
+//   MMA warp 12 (1 thread) stage-1 products of line i, then stage-2 products
+//                         of line i-1; the DFT-64 operand G lives in tensor
+//                         memory (the A operand), so the tensor core reads
+//                         only the line's operand from shared memory
+//   epilogue-1 warps 4-7  stage-1 accumulators (TMEM) -> re/im pairs -> times
+//                         W4096^(n2 k1) 2^-10 (one table, the scale change
+//                         between the stages folded in) -> stage-2 operand in
+//                         the same operand buffer
+//   epilogue-2 warps 8-11 stage-2 accumulators -> unscaled X, streamed out
+// Two accumulator slots per stage (TMEM columns 128-383; G in 0-127), three
+// operand buffers: while the tensor core runs one line, the converter, the
+// two epilogues and the loads work on up to four others.  Every wait is
+// bounded by the global timer; a wait that gives up sets a CTA-wide abort
+// flag, each warp group leaves its loop together (barrier with an OR), the
+// MMA thread waits (bounded) for its MMAs, and the CTA frees its TMEM.
 #include "capi_internal.h"
 #include "fft_common.cuh"
 #include "tcgen05.cuh"
@@ -50,17 +63,11 @@ constexpr int TC_R = 64;
 constexpr float TC_GSCALE = 16.0f;  // FP16 split: G stored as 16 * DFT-64
 constexpr int TC_LINE_EXP = 14;     // FP16 split: line scaled so |max| < 2^14
 
-// shared-memory byte offsets from a 1024-byte aligned base (dynamic)
-constexpr uint32_t SM_G0 = 0;          // G hi (or bf16) : 128 x 128 halves = 32 KB
-constexpr uint32_t SM_G1 = 32768;      // G lo
-
 // Operand layouts: 128-byte swizzle (1024-byte atoms of 8 rows x 128 bytes,
 // 16-byte chunk c of row r stored at chunk c ^ (r % 8)), so that the eight
 // threads of a quarter-warp storing one 128-byte row hit distinct banks.
-//  G  (A, K-major):  rows m = 2k+b (128), K = 2n+a (128) = 2 atoms of 64
 //  B1 (B, MN-major): rows = K (128), N = n2 (64 = one 128-byte row)
 //  B2 (B, K-major):  rows n = k1 (64), K = 2*n2+a (128) = 2 atoms of 64
-constexpr uint32_t G_KATOM = 16384;   // 16 row groups x 1024
 constexpr uint32_t B2_KATOM = 8192;   //  8 row groups x 1024
 constexpr uint32_t ATOM_SBO = 1024;   // stride of 8-row groups
 
@@ -75,10 +82,11 @@ __host__ __device__ constexpr uint32_t kmaj_off(uint32_t row, uint32_t kk, uint3
 __host__ __device__ constexpr uint32_t mnmaj_off(uint32_t nn, uint32_t kk) {
     return sw128(kk, nn / 8) + (nn % 8) * 2;
 }
-__host__ __device__ constexpr uint32_t g_off(int m, int kk) { return kmaj_off(m, kk, G_KATOM); }
 
-// Tables: G planes (hi, lo with the 16x scale; bf16 unscaled) in the exact
-// shared-memory image, and T[m] = W4096^m; all from FP64 sincospi.
+// Tables (FP64 sincospi): G = realified DFT-64 as plain row-major 16-bit
+// planes (row m = 2k+b, column kk = 2n+a; FP16 hi and lo of 16 * G, and
+// BF16 of G) -- the image each lane stores into tensor memory -- and
+// T[m] = W4096^m.
 __global__ void k_tc_tables(__half* g_hi, __half* g_lo, __nv_bfloat16* g_bf, float2* tw) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;  // 0 .. 128*128-1
     if (idx < 128 * 128) {
@@ -88,12 +96,11 @@ __global__ void k_tc_tables(__half* g_hi, __half* g_lo, __nv_bfloat16* g_bf, flo
         sincospi(-2.0 * (double)((n * k) % TC_R) / (double)TC_R, &s, &c);  // W64^(nk) = c + i s
         // out re = c*xr - s*xi ; out im = s*xr + c*xi
         const double gv = (b == 0) ? (a == 0 ? c : -s) : (a == 0 ? s : c);
-        const uint32_t o = g_off(m, kk) / 2;
         const float gs = (float)(gv * TC_GSCALE);
         const __half h = __float2half_rn(gs);
-        g_hi[o] = h;
-        g_lo[o] = __float2half_rn(gs - __half2float(h));
-        g_bf[o] = __float2bfloat16_rn((float)gv);
+        g_hi[idx] = h;
+        g_lo[idx] = __float2half_rn(gs - __half2float(h));
+        g_bf[idx] = __float2bfloat16_rn((float)gv);
     }
     if (idx < TC_N) {
         double s, c;
@@ -110,58 +117,30 @@ __device__ __forceinline__ float line_scale(float mx) {
     return ldexpf(1.f, TC_LINE_EXP - e);
 }
 
-// ---- four pipelines per CTA -------------------------------------------------
-//
-// One CTA of 512 threads per SM holds the DFT-64 operand once and runs four
-// independent 128-thread pipelines, each with its own line, B operand buffers
-// (32 KB), TMEM columns (D1, D2), commit mbarrier and named barrier: four
-// lines in flight per SM where two CTAs of one pipeline each hold two (and
-// two copies of the operand).  A pipeline's four warps cover the 128 TMEM
-// lanes, each walking both 32-column halves of D1 and D2; lines are loaded
-// directly into registers, the pipeline's next line prefetched into L2 one
-// line ahead (split 33.1 -> 34.6 M, BF16 45.9 -> 48.9 M transforms/s).
-constexpr int TQ_PIPES = 4, TQ_PT = 128, TQ_THREADS = TQ_PIPES * TQ_PT;
-constexpr uint32_t TQ_B = 65536, TQ_BSTRIDE = 32768;          // pipeline p: B hi at TQ_B + p*TQ_BSTRIDE, lo +16 KB
-constexpr uint32_t TQ_T1 = TQ_B + TQ_PIPES * TQ_BSTRIDE;      // W4096^(i*k1), i < 16: 8 KB
-constexpr uint32_t TQ_T0 = TQ_T1 + 8192;                      // W4096^(16*j*k1), j < 4: 2 KB
-constexpr uint32_t TQ_SMEM = TQ_T0 + 2048 + 1024;             // + alignment slack
-
+// 8 FP32 values -> one 16-byte chunk of the operand (hi plane at b, lo plane
+// at b + 16 KB for the split; bf16 otherwise)
 template <bool SPLIT>
-__device__ __forceinline__ void store_chunk_b(uint8_t* bhi, uint32_t off, const float (&x)[8]) {
+__device__ __forceinline__ void store_chunk_b(uint8_t* b, uint32_t off, const float (&x)[8]) {
     if constexpr (SPLIT) {
-        __align__(16) __half hi[8];
-        __align__(16) __half lo[8];
+        uint32_t hi[4], lo[4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            hi[i] = __float2half_rn(x[i]);
-            lo[i] = __float2half_rn(x[i] - __half2float(hi[i]));
+        for (int i = 0; i < 4; ++i) {
+            const __half2 h = __floats2half2_rn(x[2 * i], x[2 * i + 1]);
+            const float2 hf = __half22float2(h);
+            const __half2 l = __floats2half2_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y);
+            hi[i] = *reinterpret_cast<const uint32_t*>(&h);
+            lo[i] = *reinterpret_cast<const uint32_t*>(&l);
         }
-        *reinterpret_cast<uint4*>(bhi + off) = *reinterpret_cast<const uint4*>(hi);
-        *reinterpret_cast<uint4*>(bhi + 16384 + off) = *reinterpret_cast<const uint4*>(lo);
+        *reinterpret_cast<uint4*>(b + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4*>(b + 16384 + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
     } else {
-        __align__(16) __nv_bfloat16 bf[8];
+        uint32_t w[4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) bf[i] = __float2bfloat16_rn(x[i]);
-        *reinterpret_cast<uint4*>(bhi + off) = *reinterpret_cast<const uint4*>(bf);
-    }
-}
-
-// D (+)= G * B over K = 128 with this pipeline's B planes at b_addr (lo +16 KB)
-template <bool SPLIT, bool B_MN>
-__device__ __forceinline__ void issue_product_q(uint32_t d_tmem, uint32_t g_addr, uint32_t b_addr, uint32_t idesc) {
-    constexpr int NPROD = SPLIT ? 3 : 1;
-#pragma unroll
-    for (int pr = 0; pr < NPROD; ++pr) {
-        const uint32_t ga = g_addr + (pr == 2 ? SM_G1 : SM_G0);
-        const uint32_t bb = b_addr + (pr == 1 ? 16384u : 0u);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const uint64_t ad = tc::smem_desc(ga + (j / 4) * G_KATOM + (j % 4) * 32, 16, ATOM_SBO, tc::LAYOUT_SW128);
-            const uint64_t bd =
-                B_MN ? tc::smem_desc(bb + 2 * j * ATOM_SBO, 16384, ATOM_SBO, tc::LAYOUT_SW128)
-                     : tc::smem_desc(bb + (j / 4) * B2_KATOM + (j % 4) * 32, 16, ATOM_SBO, tc::LAYOUT_SW128);
-            tc::mma_f16_ss(d_tmem, ad, bd, idesc, (pr > 0 || j > 0) ? 1u : 0u);
+        for (int i = 0; i < 4; ++i) {
+            const __nv_bfloat162 h = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+            w[i] = *reinterpret_cast<const uint32_t*>(&h);
         }
+        *reinterpret_cast<uint4*>(b + off) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
@@ -170,226 +149,352 @@ __device__ __forceinline__ void prefetch_l2(const void* g, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g), "r"(bytes) : "memory");
 }
 
-__device__ __forceinline__ void pipe_sync(int p) {
-    asm volatile("bar.sync %0, %1;" ::"r"(1 + p), "r"(TQ_PT) : "memory");
+// ---- the warp-specialised kernel --------------------------------------------
+
+constexpr int TW_CONV = 0, TW_EPI1 = 4, TW_EPI2 = 8, TW_MMA = 12;  // first warp of each role
+constexpr int TW_THREADS = 13 * 32;
+constexpr int TW_NOP = 3;    // operand buffers (stage-1 operand, then the stage-2 operand of the same line)
+constexpr int TW_ND = 2;     // accumulator slots per stage
+constexpr int TW_NS1 = 8;    // line-scale ring (the converter runs at most 5 lines ahead of epilogue 2)
+constexpr uint32_t TW_OPB = 32768;                       // one operand buffer: hi 16 KB + lo 16 KB
+constexpr uint32_t TW_TAB = TW_NOP * TW_OPB;             // twiddle table: 4096 float2 = 32 KB
+constexpr uint32_t TW_SMEM = TW_TAB + 32768 + 1024;      // + alignment slack
+constexpr uint32_t TW_GCOL = 0, TW_D1COL = 128, TW_D2COL = 256;  // TMEM columns
+constexpr int TW_BAR_CONV = 1, TW_BAR_EPI1 = 2, TW_BAR_EPI2 = 3;  // named barriers (0 is __syncthreads)
+
+// bounded wait that also leaves when another role has aborted the CTA
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (*abort) return false;
+        if (globaltimer_ns() - t0 > WAIT_LIMIT_NS) {
+            *abort = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+// lane m of the calling warp's quarter: pairs (row 2k, row 2k+1) of 32
+// accumulator columns into 16 complex values z[i] (column 16*b + i of the
+// half), scaled by s
+__device__ __forceinline__ void pair_half(const float (&v)[32], int bsel, float s, float2 (&z)[16]) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const float send = bsel ? v[i] : v[16 + i];
+        const float r = __shfl_xor_sync(0xffffffffu, send, 1);
+        z[i] = bsel ? make_float2(r * s, v[16 + i] * s) : make_float2(v[i] * s, r * s);
+    }
 }
 
 template <bool SPLIT, bool INV>
-__global__ void __launch_bounds__(TQ_THREADS, 1)
-    k_fft4096_tcq(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
-                  const uint4* __restrict__ gimg, const float2* __restrict__ tw, int* dev_err) {
+__global__ void __launch_bounds__(TW_THREADS, 1)
+    k_fft4096_tcw(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
+                  const uint4* __restrict__ gplain, const float2* __restrict__ tw, int* dev_err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    __shared__ __align__(8) uint64_t mbar[TQ_PIPES];
+    __shared__ __align__(8) uint64_t op_full1[TW_NOP], op_full2[TW_NOP], op_empty[TW_NOP];
+    __shared__ __align__(8) uint64_t d1_full[TW_ND], d1_empty[TW_ND], d2_full[TW_ND], d2_empty[TW_ND];
+    __shared__ __align__(8) uint64_t s1_full[TW_NS1], drain;
+    __shared__ float s1ring[TW_NS1];
+    __shared__ float red[2][4];
     __shared__ uint32_t tmem_base_sh;
-    __shared__ float red1[TQ_PIPES][4];
-    __shared__ int abort_sh[TQ_PIPES];
+    __shared__ int abort_flag;
+    volatile int* abort_sh = &abort_flag;
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int p = warp >> 2;              // pipeline
-    const int q = warp & 3;               // this warp's TMEM lane quarter
-    const int ptid = tid & (TQ_PT - 1);   // thread within the pipeline
     uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const uint32_t sbase = smem_u32(smem);
+    float2* tab = reinterpret_cast<float2*>(smem + TW_TAB);
     constexpr uint32_t FMT = SPLIT ? 0u : 1u;
     constexpr uint32_t IDESC1 = tc::idesc_f16(FMT, 1u, 128, 64);
     constexpr uint32_t IDESC2 = tc::idesc_f16(FMT, 0u, 128, 64);
+    const long long G = gridDim.x;
+    const long long nlines = batch > (long long)blockIdx.x ? (batch - blockIdx.x + G - 1) / G : 0;
 
-    constexpr int GWORDS = (SPLIT ? 65536 : 32768) / 16;
-    for (int i = tid; i < GWORDS; i += TQ_THREADS) reinterpret_cast<uint4*>(smem)[i] = __ldg(gimg + i);
-    float2* t1 = reinterpret_cast<float2*>(smem + TQ_T1);
-    float2* t0 = reinterpret_cast<float2*>(smem + TQ_T0);
-    for (int i = tid; i < 16 * 64; i += TQ_THREADS) t1[i] = __ldg(tw + ((i >> 6) * (i & 63)));
-    for (int i = tid; i < 4 * 64; i += TQ_THREADS) t0[i] = __ldg(tw + (16 * (i >> 6) * (i & 63)));
-    if (tid < TQ_PIPES) {
-        mbar_init(&mbar[tid], 1);
-        abort_sh[tid] = 0;
+    // T[n2*64 + k1] = W4096^(n2 k1) (times 2^-10 for the split: the stage-2
+    // operand is D1 / (16 s1) * W * s1 / 64)
+    for (int i = tid; i < TC_N; i += TW_THREADS) {
+        const float2 w = __ldg(tw + (((i >> 6) * (i & 63)) & (TC_N - 1)));
+        const float sc = SPLIT ? 0.0009765625f : 1.f;
+        tab[i] = make_float2(w.x * sc, w.y * sc);
     }
-    if (warp == 0) {
+    if (tid == 0) {
+        for (int j = 0; j < TW_NOP; ++j) {
+            mbar_init(&op_full1[j], 128);
+            mbar_init(&op_full2[j], 128);
+            mbar_init(&op_empty[j], 1);
+        }
+        for (int j = 0; j < TW_ND; ++j) {
+            mbar_init(&d1_full[j], 1);
+            mbar_init(&d1_empty[j], 128);
+            mbar_init(&d2_full[j], 1);
+            mbar_init(&d2_empty[j], 128);
+        }
+        for (int j = 0; j < TW_NS1; ++j) mbar_init(&s1_full[j], 1);
+        mbar_init(&drain, 1);
+        abort_flag = 0;
+        fence_proxy_async_smem();
+    }
+    if (warp == TW_MMA) {
         tc::tmem_alloc(&tmem_base_sh, 512);
         tc::tmem_relinquish();
     }
-    fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t d1 = tmem_base_sh + (uint32_t)p * 128u, d2 = d1 + 64u;
-    uint8_t* bp = smem + TQ_B + (uint32_t)p * TQ_BSTRIDE;
-    const uint32_t baddr = sbase + TQ_B + (uint32_t)p * TQ_BSTRIDE;
+    const uint32_t tbase = tmem_base_sh;
 
-    const int m = 32 * q + lane;  // TMEM lane = D row = 2k + b
-    const int kk_ = m >> 1, bsel = m & 1;
-    const uint32_t lane_off = (uint32_t)(32 * q) << 16;
-
-    uint32_t phase = 0;
-    bool aborted = false;
-    const long long fstep = (long long)gridDim.x * TQ_PIPES;
-    for (long long f = (long long)blockIdx.x * TQ_PIPES + p; f < batch; f += fstep) {
-        // this pipeline's next line to L2 while this one goes through both stages
-        if (ptid == 0 && f + fstep < batch) prefetch_l2(in + (size_t)(f + fstep) * TC_N, TC_N * sizeof(float2));
-        // ---- the line, its scale, the stage-1 operand (MN-major) ----
-        float4 cur[16];
-        const float4* src = reinterpret_cast<const float4*>(in + (size_t)f * TC_N);
-#pragma unroll
-        for (int it = 0; it < 4; ++it)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) cur[4 * it + j] = __ldcs(src + 4 * (ptid + TQ_PT * it) + j);
-        if constexpr (INV) {
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                cur[i].y = -cur[i].y;
-                cur[i].w = -cur[i].w;
-            }
-        }
-        float s1 = 1.f;
-        if constexpr (SPLIT) {
-            float mx = 0.f;
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-                mx = fmaxf(mx, fmaxf(fmaxf(fabsf(cur[i].x), fabsf(cur[i].y)), fmaxf(fabsf(cur[i].z), fabsf(cur[i].w))));
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            if (lane == 0) red1[p][q] = mx;
-            pipe_sync(p);
-            s1 = line_scale(fmaxf(fmaxf(red1[p][0], red1[p][1]), fmaxf(red1[p][2], red1[p][3])));
-        }
-#pragma unroll
-        for (int it = 0; it < 4; ++it) {
-            const int item = ptid + TQ_PT * it;  // (n1, c): n2 = 8c .. 8c+7
-            const int n1 = item >> 3, c = item & 7;
-            float re[8], im[8];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const float4 v = cur[4 * it + j];
-                re[2 * j] = v.x * s1;
-                im[2 * j] = v.y * s1;
-                re[2 * j + 1] = v.z * s1;
-                im[2 * j + 1] = v.w * s1;
-            }
-            store_chunk_b<SPLIT>(bp, mnmaj_off(8 * c, 2 * n1), re);
-            store_chunk_b<SPLIT>(bp, mnmaj_off(8 * c, 2 * n1 + 1), im);
-        }
-        fence_proxy_async_smem();
-        tc::fence_before_sync();
-        pipe_sync(p);
-
-        // ---- stage 1 ----
-        if (ptid == 0) {
-            tc::fence_after_sync();
-            issue_product_q<SPLIT, true>(d1, sbase, baddr, IDESC1);
-            tc::mma_commit(&mbar[p]);
-            if (!mbar_wait(&mbar[p], phase)) abort_sh[p] = 1;
-        }
-        phase ^= 1u;
-        pipe_sync(p);
-        if (abort_sh[p]) {
-            aborted = true;
-            break;
-        }
-        tc::fence_after_sync();
-
-        // ---- epilogue 1: unscale, pair re/im, twiddle, scale, stage-2 operand (K-major) ----
-        const float inv1 = 1.f / ((SPLIT ? TC_GSCALE : 1.f) * s1);
-        const float s2 = SPLIT ? s1 * (1.f / 64.f) : 1.f;
+    // G into tensor memory: lane m holds row m (hi in columns 0-63, lo in 64-127)
+    if (warp >= TW_EPI1 && warp < TW_EPI1 + 4) {
+        const int m = 32 * (warp & 3) + lane;
+        const uint32_t lane_off = (uint32_t)(32 * (warp & 3)) << 16;
 #pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-            float2 z[16];
-            {
-                float v[32];
-                tc::tmem_ld32(d1 + lane_off + 32 * h, v);
+        for (int pl = 0; pl < (SPLIT ? 2 : 1); ++pl) {
+            // plane pl: hi (SPLIT) / bf16 at gplain, lo at gplain + 128*128 halves
+            const uint4* row = gplain + (size_t)pl * 2048 + (size_t)m * 16;
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const float send = bsel ? v[i] : v[16 + i];
-                    const float r = __shfl_xor_sync(0xffffffffu, send, 1);
-                    z[i] = bsel ? make_float2(r * inv1, v[16 + i] * inv1) : make_float2(v[i] * inv1, r * inv1);
+            for (int h = 0; h < 2; ++h) {
+                uint32_t r[32];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const uint4 u = __ldg(row + 8 * h + q);
+                    r[4 * q] = u.x;
+                    r[4 * q + 1] = u.y;
+                    r[4 * q + 2] = u.z;
+                    r[4 * q + 3] = u.w;
                 }
-            }
-            const int n2_0 = 32 * h + 16 * bsel;
-            const float2 w0 = t0[(n2_0 >> 4) * 64 + kk_];
-#pragma unroll
-            for (int i = 0; i < 16; ++i) z[i] = cmul(z[i], cmul(w0, t1[i * 64 + kk_]));
-#pragma unroll
-            for (int qq = 0; qq < 4; ++qq) {
-                float x[8];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    x[2 * j] = z[4 * qq + j].x * s2;
-                    x[2 * j + 1] = z[4 * qq + j].y * s2;
-                }
-                store_chunk_b<SPLIT>(bp, kmaj_off(kk_, 2 * (n2_0 + 4 * qq), B2_KATOM), x);
+                tc::tmem_st32(tbase + lane_off + TW_GCOL + 64 * pl + 32 * h, r);
             }
         }
-        fence_proxy_async_smem();
-        tc::fence_before_sync();
-        pipe_sync(p);
-
-        // ---- stage 2 ----
-        if (ptid == 0) {
-            tc::fence_after_sync();
-            issue_product_q<SPLIT, false>(d2, sbase, baddr, IDESC2);
-            tc::mma_commit(&mbar[p]);
-            if (!mbar_wait(&mbar[p], phase)) abort_sh[p] = 1;
-        }
-        phase ^= 1u;
-        pipe_sync(p);
-        if (abort_sh[p]) {
-            aborted = true;
-            break;
-        }
-        tc::fence_after_sync();
-
-        // ---- epilogue 2: unscale, pair re/im, store X[k1 + 64 k2] ----
-        const float inv2 = (INV ? 1.f / (float)TC_N : 1.f) / ((SPLIT ? TC_GSCALE : 1.f) * s2);
-#pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-            float v[32];
-            tc::tmem_ld32(d2 + lane_off + 32 * h, v);
-            float4 o[8];
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                const float send = bsel ? v[i] : v[16 + i];
-                const float r = __shfl_xor_sync(0xffffffffu, send, 1);
-                float2 y = bsel ? make_float2(r * inv2, v[16 + i] * inv2) : make_float2(v[i] * inv2, r * inv2);
-                if constexpr (INV) y.y = -y.y;
-                if (i & 1) {
-                    o[i >> 1].z = y.x;
-                    o[i >> 1].w = y.y;
-                } else {
-                    o[i >> 1].x = y.x;
-                    o[i >> 1].y = y.y;
-                }
-            }
-            const int k1_0 = 32 * h + 16 * bsel;  // k2 = kk_
-            float4* dst = reinterpret_cast<float4*>(out + (size_t)f * TC_N + TC_R * kk_ + k1_0);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) __stcs(dst + i, o[i]);
-        }
-        tc::fence_before_sync();
-        pipe_sync(p);  // this pipeline's TMEM columns and B buffers are free for its next line
-    }
-
-    if (aborted && ptid == 0) {
-        report_device_error(dev_err, DEV_ERR_MMA_TIMEOUT);
-        mbar_wait(&mbar[p], phase ^ 1u);  // bounded: let an MMA still in flight finish
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) {
+    tc::fence_after_sync();
+
+    if (warp < TW_CONV + 4) {
+        // ---------------- converter: the stage-1 operand of each line ----------------
+        const int ctid = tid;
+#pragma unroll 1
+        for (long long i = 0; i < nlines; ++i) {
+            const long long f = blockIdx.x + i * G;
+            const int o = (int)(i % TW_NOP);
+            if (ctid == 0 && i + 2 < nlines) prefetch_l2(in + (size_t)(f + 2 * G) * TC_N, TC_N * sizeof(float2));
+            float4 cur[16];
+            const float4* src = reinterpret_cast<const float4*>(in + (size_t)f * TC_N);
+#pragma unroll
+            for (int it = 0; it < 4; ++it)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) cur[4 * it + j] = __ldcs(src + 4 * (ctid + 128 * it) + j);
+            if constexpr (INV) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    cur[q].y = -cur[q].y;
+                    cur[q].w = -cur[q].w;
+                }
+            }
+            if constexpr (SPLIT) {
+                float mx = 0.f;
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    mx = fmaxf(mx, fmaxf(fmaxf(fabsf(cur[q].x), fabsf(cur[q].y)), fmaxf(fabsf(cur[q].z), fabsf(cur[q].w))));
+#pragma unroll
+                for (int sh = 16; sh > 0; sh >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, sh));
+                if (lane == 0) red[i & 1][warp] = mx;
+            }
+            // the operand buffer is free once the previous user's stage-2 products are done
+            bool ok = true;
+            if (ctid == 0) ok = wait_or_abort(&op_empty[o], (uint32_t)(((i / TW_NOP) & 1) ^ 1), abort_sh);
+            if (bar_or(TW_BAR_CONV, 128, !ok)) break;
+            float s1 = 1.f;
+            if constexpr (SPLIT) s1 = line_scale(fmaxf(fmaxf(red[i & 1][0], red[i & 1][1]), fmaxf(red[i & 1][2], red[i & 1][3])));
+            uint8_t* bp = smem + (uint32_t)o * TW_OPB;
+#pragma unroll
+            for (int it = 0; it < 4; ++it) {
+                const int item = ctid + 128 * it;  // (n1, c): n2 = 8c .. 8c+7
+                const int n1 = item >> 3, c = item & 7;
+                float re[8], im[8];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float4 v = cur[4 * it + j];
+                    re[2 * j] = v.x * s1;
+                    im[2 * j] = v.y * s1;
+                    re[2 * j + 1] = v.z * s1;
+                    im[2 * j + 1] = v.w * s1;
+                }
+                store_chunk_b<SPLIT>(bp, mnmaj_off(8 * c, 2 * n1), re);
+                store_chunk_b<SPLIT>(bp, mnmaj_off(8 * c, 2 * n1 + 1), im);
+            }
+            if (ctid == 0) {
+                s1ring[i % TW_NS1] = s1;
+                mbar_arrive(&s1_full[i % TW_NS1]);
+            }
+            fence_proxy_async_smem();  // the operand's generic writes before the tensor core reads them
+            mbar_arrive(&op_full1[o]);
+        }
+    } else if (warp < TW_EPI1 + 4) {
+        // ---------------- epilogue 1: twiddle and the stage-2 operand ----------------
+        const int q = warp & 3, m = 32 * q + lane;
+        const int k1 = m >> 1, bsel = m & 1;
+        const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+#pragma unroll 1
+        for (long long i = 0; i < nlines; ++i) {
+            const int d = (int)(i % TW_ND), o = (int)(i % TW_NOP);
+            bool ok = true;
+            if (m == 0) ok = wait_or_abort(&d1_full[d], (uint32_t)((i / TW_ND) & 1), abort_sh);
+            if (bar_or(TW_BAR_EPI1, 128, !ok)) break;
+            tc::fence_after_sync();
+            float v0[32], v1[32];
+            const uint32_t dcol = tbase + lane_off + TW_D1COL + 64 * d;
+            tc::tmem_ld32(dcol, v0);
+            tc::tmem_ld32(dcol + 32, v1);
+            tc::fence_before_sync();
+            mbar_arrive(&d1_empty[d]);  // the accumulator slot may take the next line
+            uint8_t* bp = smem + (uint32_t)o * TW_OPB;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                float2 z[16];
+                pair_half(h ? v1 : v0, bsel, 1.f, z);
+                const int n2_0 = 32 * h + 16 * bsel;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) z[j] = cmul(z[j], tab[(n2_0 + j) * 64 + k1]);
+#pragma unroll
+                for (int qq = 0; qq < 4; ++qq) {
+                    float x[8];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        x[2 * j] = z[4 * qq + j].x;
+                        x[2 * j + 1] = z[4 * qq + j].y;
+                    }
+                    store_chunk_b<SPLIT>(bp, kmaj_off(k1, 2 * (n2_0 + 4 * qq), B2_KATOM), x);
+                }
+            }
+            fence_proxy_async_smem();
+            mbar_arrive(&op_full2[o]);
+        }
+    } else if (warp < TW_EPI2 + 4) {
+        // ---------------- epilogue 2: X out ----------------
+        const int q = warp & 3, m = 32 * q + lane;
+        const int k2 = m >> 1, bsel = m & 1;
+        const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+#pragma unroll 1
+        for (long long i = 0; i < nlines; ++i) {
+            const long long f = blockIdx.x + i * G;
+            const int d = (int)(i % TW_ND);
+            bool ok = true;
+            if (m == 0)
+                ok = wait_or_abort(&d2_full[d], (uint32_t)((i / TW_ND) & 1), abort_sh) &&
+                     wait_or_abort(&s1_full[i % TW_NS1], (uint32_t)((i / TW_NS1) & 1), abort_sh);
+            if (bar_or(TW_BAR_EPI2, 128, !ok)) break;
+            tc::fence_after_sync();
+            // X = D2 / (16 s2), s2 = s1 / 64 (split); X = D2 (bf16)
+            const float s1 = s1ring[i % TW_NS1];
+            const float sc = (INV ? 1.f / (float)TC_N : 1.f) * (SPLIT ? 4.f / s1 : 1.f);
+            float v0[32], v1[32];
+            const uint32_t dcol = tbase + lane_off + TW_D2COL + 64 * d;
+            tc::tmem_ld32(dcol, v0);
+            tc::tmem_ld32(dcol + 32, v1);
+            tc::fence_before_sync();
+            mbar_arrive(&d2_empty[d]);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                float2 z[16];
+                pair_half(h ? v1 : v0, bsel, sc, z);
+                const int k1_0 = 32 * h + 16 * bsel;
+                float4* dst = reinterpret_cast<float4*>(out + (size_t)f * TC_N + TC_R * k2 + k1_0);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    float4 o4 = make_float4(z[2 * j].x, z[2 * j].y, z[2 * j + 1].x, z[2 * j + 1].y);
+                    if constexpr (INV) {
+                        o4.y = -o4.y;
+                        o4.w = -o4.w;
+                    }
+                    __stcs(dst + j, o4);
+                }
+            }
+        }
+    } else if (warp == TW_MMA && lane == 0) {
+        // ---------------- MMA issue: stage 1 of line i, stage 2 of line i - 1 ----------------
+        constexpr int NPROD = SPLIT ? 3 : 1;
+        const uint32_t g_hi = tbase + TW_GCOL, g_lo = g_hi + 64;
+        bool aborted = false;
+#pragma unroll 1
+        for (long long i = 0; i <= nlines && !aborted; ++i) {
+            if (i < nlines) {
+                const int o = (int)(i % TW_NOP), d = (int)(i % TW_ND);
+                if (!wait_or_abort(&op_full1[o], (uint32_t)((i / TW_NOP) & 1), abort_sh) ||
+                    !wait_or_abort(&d1_empty[d], (uint32_t)(((i / TW_ND) & 1) ^ 1), abort_sh)) {
+                    aborted = true;
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t bb = sbase + (uint32_t)o * TW_OPB;
+                const uint32_t dd = tbase + TW_D1COL + 64 * d;
+#pragma unroll
+                for (int pr = 0; pr < NPROD; ++pr) {
+                    const uint32_t ga = pr == 2 ? g_lo : g_hi;
+                    const uint32_t bpl = bb + (pr == 1 ? 16384u : 0u);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                        tc::mma_f16_ts(dd, ga + 8 * j,
+                                       tc::smem_desc(bpl + 2 * j * ATOM_SBO, 16384, ATOM_SBO, tc::LAYOUT_SW128),
+                                       IDESC1, (pr > 0 || j > 0) ? 1u : 0u);
+                }
+                tc::mma_commit(&d1_full[d]);
+            }
+            if (i >= 1) {
+                const long long k = i - 1;
+                const int o = (int)(k % TW_NOP), d = (int)(k % TW_ND);
+                if (!wait_or_abort(&op_full2[o], (uint32_t)((k / TW_NOP) & 1), abort_sh) ||
+                    !wait_or_abort(&d2_empty[d], (uint32_t)(((k / TW_ND) & 1) ^ 1), abort_sh)) {
+                    aborted = true;
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t bb = sbase + (uint32_t)o * TW_OPB;
+                const uint32_t dd = tbase + TW_D2COL + 64 * d;
+#pragma unroll
+                for (int pr = 0; pr < NPROD; ++pr) {
+                    const uint32_t ga = pr == 2 ? g_lo : g_hi;
+                    const uint32_t bpl = bb + (pr == 1 ? 16384u : 0u);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                        tc::mma_f16_ts(dd, ga + 8 * j,
+                                       tc::smem_desc(bpl + (j / 4) * B2_KATOM + (j % 4) * 32, 16, ATOM_SBO,
+                                                     tc::LAYOUT_SW128),
+                                       IDESC2, (pr > 0 || j > 0) ? 1u : 0u);
+                }
+                tc::mma_commit(&d2_full[d]);
+                tc::mma_commit(&op_empty[o]);
+            }
+        }
+        if (aborted) {
+            // every MMA this thread issued completes before the CTA frees its tensor memory
+            tc::mma_commit(&drain);
+            mbar_wait(&drain, 0);
+        }
+    }
+
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0 && abort_flag) report_device_error(dev_err, DEV_ERR_MMA_TIMEOUT);
+    if (warp == TW_MMA) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem_base_sh, 512);
+        tc::tmem_dealloc(tbase, 512);
     }
 }
 
 template <bool SPLIT, bool INV>
-cudaError_t launch_tcq(const float2* in, float2* out, long long batch, const uint4* gimg, const float2* tw,
+cudaError_t launch_tcw(const float2* in, float2* out, long long batch, const uint4* gplain, const float2* tw,
                        int* dev_err, int sms, cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(k_fft4096_tcq<SPLIT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         TQ_SMEM);
+    cudaError_t e = cudaFuncSetAttribute(k_fft4096_tcw<SPLIT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TW_SMEM);
     if (e != cudaSuccess) return e;
-    long long blocks = (batch + TQ_PIPES - 1) / TQ_PIPES;
+    long long blocks = batch;
     if (blocks > sms) blocks = sms;
     if (blocks <= 0) return cudaSuccess;
-    k_fft4096_tcq<SPLIT, INV><<<(unsigned)blocks, TQ_THREADS, TQ_SMEM, s>>>(in, out, batch, gimg, tw, dev_err);
+    k_fft4096_tcw<SPLIT, INV><<<(unsigned)blocks, TW_THREADS, TW_SMEM, s>>>(in, out, batch, gplain, tw, dev_err);
     return cudaGetLastError();
 }
 
@@ -432,11 +537,11 @@ int tc_launch(mfft_plan* p, const float2* in, float2* out, int64_t batch, int di
     cudaError_t e;
     const bool inv = (direction == MFFT_INVERSE);
     if (variant == MFFT_TC_FP16_SPLIT3)
-        e = inv ? launch_tcq<true, true>(in, out, batch, g_split, p->tc.tw, err, sms, s)
-                : launch_tcq<true, false>(in, out, batch, g_split, p->tc.tw, err, sms, s);
+        e = inv ? launch_tcw<true, true>(in, out, batch, g_split, p->tc.tw, err, sms, s)
+                : launch_tcw<true, false>(in, out, batch, g_split, p->tc.tw, err, sms, s);
     else
-        e = inv ? launch_tcq<false, true>(in, out, batch, g_bf, p->tc.tw, err, sms, s)
-                : launch_tcq<false, false>(in, out, batch, g_bf, p->tc.tw, err, sms, s);
+        e = inv ? launch_tcw<false, true>(in, out, batch, g_bf, p->tc.tw, err, sms, s)
+                : launch_tcw<false, false>(in, out, batch, g_bf, p->tc.tw, err, sms, s);
     if (e != cudaSuccess) return cuda_error(e, "tensor-core FFT launch");
     return MFFT_SUCCESS;
 }

@@ -30,6 +30,24 @@ def test_split_fp16_forward_inverse(M, batch):
     assert O.rel_rms(yi, O.truth(x, inverse=True)) < TOL_SPLIT
 
 
+@pytest.mark.parametrize("tc", ["split", "bf16"])
+def test_many_lines_per_cta(M, tc):
+    """3000 lines: about 20 per persistent CTA, so every ring of the
+    warp-specialised kernel (operand buffers, accumulator slots, line scales)
+    wraps several times; every line against FP64."""
+    x = O.normal_c64((3000, N), seed=612)
+    x[1234] *= np.float32(1e12)  # one line far from the others: its own scale
+    variant = M.TC_FP16_SPLIT3 if tc == "split" else M.TC_BF16
+    bar = TOL_SPLIT if tc == "split" else TOL_BF16
+    f = M.MetalFFT(N)
+    y = f.forward_batch(x, tc_variant=variant)
+    ref = O.truth(x)
+    err = np.array([O.rel_rms(y[i:i + 1], ref[i:i + 1]) for i in range(0, 3000, 1)])
+    assert err.max() < bar, (int(err.argmax()), err.max())
+    yi = f.inverse_batch(x, tc_variant=variant)
+    assert O.rel_rms(yi[::7], O.truth(x[::7], inverse=True)) < bar
+
+
 def test_bf16_variant(M):
     x = O.normal_c64((64, N), seed=77)
     y = M.MetalFFT(N).forward_batch(x, tc_variant=M.TC_BF16)
