@@ -228,8 +228,9 @@ class _Desc(ctypes.Structure):
 
 
 class MixedBatch:
-    """Transforms of several sizes in a few launches of the persistent item
-    kernel (no reference counterpart).  sizes_counts: [(n, count), ...];
+    """Transforms of several sizes in one persistent launch that draws its
+    work items from a device-side queue (no reference counterpart).
+    sizes_counts: [(n, count), ...];
     transforms of a class are stored back to back, classes one after another
     in the given order."""
 

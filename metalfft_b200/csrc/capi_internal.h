@@ -1,6 +1,7 @@
 // capi_internal.h -- handle layouts and helpers shared by the C-ABI sources.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <functional>
@@ -133,6 +134,11 @@ int fourstep_tables(mfft_ctx* ctx, int64_t n, float2** out);
 // (FSQ_COLS or FSQ_ROWS) of them over nb contiguous transforms of 2^logn
 // points: in / out / scratch are the first transform's data (fsqueue.h).
 bool fsq_tma_size(int logn);
+// Tensor map of `rows` rows of `row_points` complex values at `base`, boxes of
+// tile_cols complex columns x box_rows rows with the item tiles' swizzle (32,
+// 64 or 128 bytes for 4, 8 or 16 columns).
+bool encode_rows(CUtensorMap* map, const float2* base, uint64_t rows, uint64_t row_points, int tile_cols,
+                 int box_rows = 256);
 struct FsqTables;
 int fourstep_tma_pass(int kind, const FsqTables& tabs, const float2* in, float2* out, float2* scratch, long long nb,
                       int logn, bool inv, mfft_ctx* ctx, cudaStream_t s, int adjoint = 0);

@@ -111,13 +111,14 @@ static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
 }
 
 // `rows` rows of `row_points` complex values at `base`, as floats; boxes of
-// `tile_cols` complex columns x 256 rows, swizzled like the item tiles
-static bool encode_rows(CUtensorMap* map, const float2* base, uint64_t rows, uint64_t row_points, int tile_cols) {
+// `tile_cols` complex columns x box_rows rows, swizzled like the item tiles
+bool encode_rows(CUtensorMap* map, const float2* base, uint64_t rows, uint64_t row_points, int tile_cols,
+                 int box_rows) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
     if (!enc) return false;
     const cuuint64_t dims[2] = {2 * row_points, rows};
     const cuuint64_t strides[1] = {row_points * sizeof(float2)};
-    const cuuint32_t box[2] = {(cuuint32_t)(2 * tile_cols), 256};
+    const cuuint32_t box[2] = {(cuuint32_t)(2 * tile_cols), (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     const CUtensorMapSwizzle sw = tile_cols == 4   ? CU_TENSOR_MAP_SWIZZLE_32B
                                   : tile_cols == 8 ? CU_TENSOR_MAP_SWIZZLE_64B

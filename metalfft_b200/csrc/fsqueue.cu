@@ -438,11 +438,232 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
     }
 }
 
+// ---- one launch over the device-side descriptor queue -------------------------
+
+// the calling thread's earlier cp.async copies arrive on `bar` when they land
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+// transform index of a TMA item inside its group
+__device__ __forceinline__ long long q_group_index(const FsqQueueArgs& q, const FsqItem& it) {
+    return (q.a.xf[it.xform].off - q.groups[it.grp].off) >> it.logn;
+}
+
+// every thread: item `p`'s data into stage `st`, completion on `bar`
+// (256 arrivals: cp.async copies of every thread, or thread 0's bulk copies
+// counted in bytes plus 255 plain arrivals)
+__device__ __forceinline__ void q_issue(const FsqQueueArgs& q, int p, float2* st, uint64_t* bar, uint64_t pol) {
+    const FsqItem it = q.a.items[p];
+    if (it.grp < 0) {
+        issue(q.a, get_work(q.a, p), st, pol);
+        cp_async_mbar_arrive(bar);
+        return;
+    }
+    if (threadIdx.x != 0) {
+        mbar_arrive(bar);
+        return;
+    }
+    const FsqGroupMaps& m = q.maps[it.grp];
+    const int l1 = it.logn / 2, l2 = it.logn - l1;
+    mbar_arrive_expect_tx(bar, FSQ_POINTS * (uint32_t)sizeof(float2));
+    const long long j = q_group_index(q, it);
+    if (it.kind == FSQ_COLS) {
+        const int lc = ilog2c(FSQ_POINTS) - l1;
+        const int x = (it.index << lc) * 2;  // floats
+        const int C = 1 << lc;
+        for (int k = 0; k < (1 << l1) / TMA_BOX_ROWS; ++k)
+            tma_load_2d(st + k * TMA_BOX_ROWS * C, &m.ld, x, (int)(j << l1) + k * TMA_BOX_ROWS, bar);
+    } else {
+        // the intermediate was written by other CTAs (generic and async proxies)
+        fence_proxy_async_global();
+        const int lr = ilog2c(FSQ_POINTS) - l2;
+        const FsqXform x = q.a.xf[it.xform];
+        bulk_g2s(st, q.a.scratch + x.scratch + ((long long)it.index << (lr + l2)), FSQ_POINTS * (uint32_t)sizeof(float2),
+                 bar);
+    }
+}
+
+// thread 0: the finished tile of TMA item `it` from stage `st`
+__device__ __forceinline__ void q_tma_store(const FsqQueueArgs& q, const FsqItem& it, const float2* st) {
+    const FsqGroupMaps& m = q.maps[it.grp];
+    const int l1 = it.logn / 2, l2 = it.logn - l1;
+    const long long j = q_group_index(q, it);
+    if (it.kind == FSQ_COLS) {
+        const int lc = ilog2c(FSQ_POINTS) - l1, C = 1 << lc;
+        const int x = (it.index << lc) * 2;
+        for (int k = 0; k < (1 << l1) / TMA_BOX_ROWS; ++k)
+            tma_store_2d(&m.stc, x, (int)(j << l1) + k * TMA_BOX_ROWS, st + k * TMA_BOX_ROWS * C);
+    } else {
+        const int lr = ilog2c(FSQ_POINTS) - l2, RW = 1 << lr;
+        const int x = (it.index << lr) * 2;
+        for (int k = 0; k < (1 << l2) / TMA_BOX_ROWS; ++k)
+            tma_store_2d(&m.str, x, (int)(j << l2) + k * TMA_BOX_ROWS, st + k * TMA_BOX_ROWS * RW);
+    }
+    bulk_commit();
+}
+
+// COLS items of a transform, counted when each is done
+__device__ __forceinline__ int q_cols_needed(int logn) { return fsq_cols_items_dev(logn); }
+
+// thread 0: for a ROWS item, waits (bounded) until every COLS item of its
+// transform is counted done; other items need nothing
+__device__ __forceinline__ bool q_wait_cols(const FsqQueueArgs& q, int p) {
+    const FsqItem it = q.a.items[p];
+    if (it.kind != FSQ_ROWS) return true;
+    const int need = q_cols_needed(it.logn);
+    if (ld_acquire_gpu(q.counters + 1 + it.xform) >= need) return true;
+    const uint64_t t0 = globaltimer_ns();
+    while (ld_acquire_gpu(q.counters + 1 + it.xform) < need)
+        if (globaltimer_ns() - t0 > WAIT_LIMIT_NS) return false;
+    return true;
+}
+
+// thread 0: publish a finished COLS item of transform x (its tile stores
+// done and visible GPU-wide before the count that ROWS items acquire)
+__device__ __forceinline__ void q_publish(const FsqQueueArgs& q, int x, bool tma) {
+    if (x < 0) return;
+    if (tma) {
+        bulk_wait_all();
+        fence_proxy_async_global();
+    }
+    __threadfence();
+    atomicAdd(q.counters + 1 + x, 1);
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
+    k_fsq_queue(const __grid_constant__ FsqQueueArgs q, int* dev_err) {
+    extern __shared__ __align__(1024) unsigned char fsq_raw[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int sh_next, sh_ready;
+    float2* smem = reinterpret_cast<float2*>(fsq_raw + ((1024u - (smem_u32(fsq_raw) & 1023u)) & 1023u));
+    const int n = q.a.nitems;
+    const uint64_t pol = policy_evict_first();
+    // every item, the first included, is drawn by ticket: a CTA that draws a
+    // ROWS item knows that running CTAs hold all of its transform's COLS items
+    bool first_ok = true;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], FSQ_THREADS);
+        mbar_init(&bar[1], FSQ_THREADS);
+        fence_proxy_async_smem();
+        const int c = atomicAdd(q.counters, 1);
+        sh_next = c;
+        if (c < n) first_ok = q_wait_cols(q, c);
+    }
+    if (__syncthreads_or(!first_ok)) {
+        if (threadIdx.x == 0) report_device_error(dev_err, DEV_ERR_QUEUE_TIMEOUT);
+        return;
+    }
+    int cur = sh_next;
+    if (cur >= n) return;
+    q_issue(q, cur, smem, &bar[0], pol);
+    uint32_t ph[2] = {0u, 0u};
+    int s = 0;
+    int pending = -1;  // thread 0: transform of a finished, not yet published COLS item
+    bool pending_tma = false;
+    bool failed = false;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            q_publish(q, pending, pending_tma);
+            pending = -1;
+            const int nx = atomicAdd(q.counters, 1);
+            int ready = 1;
+            if (nx < n) {
+                const FsqItem it = q.a.items[nx];
+                if (it.kind == FSQ_ROWS)
+                    ready = ld_acquire_gpu(q.counters + 1 + it.xform) >= q_cols_needed(it.logn);
+            }
+            bulk_wait_read_all();  // the other stage is no longer read by a bulk store
+            sh_next = nx;
+            sh_ready = ready;
+        }
+        __syncthreads();
+        const int nx = sh_next;
+        const bool ready = sh_ready != 0;
+        if (nx < n && ready) q_issue(q, nx, smem + (s ^ 1) * QSTAGE, &bar[s ^ 1], pol);
+        const bool landed = mbar_wait(&bar[s], ph[s]);
+        ph[s] ^= 1u;
+        if (__syncthreads_or(!landed)) {
+            failed = true;
+            break;
+        }
+        const FsqItem it = q.a.items[cur];
+        const Work w = get_work(q.a, cur);
+        float2* st = smem + s * QSTAGE;
+        if (it.grp >= 0) {
+            compute<INV, true>(q.a, w, st);
+            fence_proxy_async_smem();  // the tile's generic writes before the bulk store reads them
+            __syncthreads();
+            if (threadIdx.x == 0) q_tma_store(q, it, st);
+        } else {
+            compute<INV>(q.a, w, st);
+            if (it.kind == FSQ_COLS) __threadfence();  // this thread's tile stores before the count
+        }
+        if (threadIdx.x == 0 && it.kind == FSQ_COLS) {
+            pending = it.xform;
+            pending_tma = it.grp >= 0;
+        }
+        if (nx < n && !ready) {
+            // a ROWS item whose columns are still in flight elsewhere: publish
+            // this CTA's own item first, then wait (bounded)
+            __syncthreads();  // every writer's fence is done
+            bool ok = true;
+            if (threadIdx.x == 0) {
+                q_publish(q, pending, pending_tma);
+                pending = -1;
+                ok = q_wait_cols(q, nx);
+            }
+            if (__syncthreads_or(!ok)) {
+                failed = true;
+                break;
+            }
+            q_issue(q, nx, smem + (s ^ 1) * QSTAGE, &bar[s ^ 1], pol);
+        }
+        __syncthreads();  // every read of stage s is done before it is refilled
+        if (nx >= n) break;
+        cur = nx;
+        s ^= 1;
+    }
+    if (threadIdx.x == 0) {
+        if (failed) {
+            report_device_error(dev_err, DEV_ERR_QUEUE_TIMEOUT);
+            // copies still in flight land before the CTA's shared memory goes away
+            mbar_wait(&bar[0], ph[0]);
+            mbar_wait(&bar[1], ph[1]);
+        } else {
+            q_publish(q, pending, pending_tma);
+        }
+        bulk_wait_all();
+    }
+}
+
 }  // namespace
+
+cudaError_t fsq_launch_queue(const FsqQueueArgs& q, bool inverse, int sms, int* dev_err, cudaStream_t s) {
+    if (q.a.nitems <= 0) return cudaSuccess;
+    long long grid = (long long)sms * FSQ_CTAS_PER_SM;
+    if (grid > q.a.nitems) grid = q.a.nitems;
+    if (inverse) k_fsq_queue<true><<<(unsigned)grid, FSQ_THREADS, QSMEM + 1024, s>>>(q, dev_err);
+    else k_fsq_queue<false><<<(unsigned)grid, FSQ_THREADS, QSMEM + 1024, s>>>(q, dev_err);
+    return cudaGetLastError();
+}
 
 cudaError_t fsq_prepare() {
     for (auto k : {k_fsq<false>, k_fsq<true>}) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, QSMEM);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+    }
+    for (auto k : {k_fsq_queue<false>, k_fsq_queue<true>}) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, QSMEM + 1024);
         if (e != cudaSuccess) return e;
         e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess) return e;

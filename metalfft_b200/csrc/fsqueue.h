@@ -36,7 +36,7 @@ struct FsqItem {
     int xform;      // four-step transform id (COLS / ROWS)
     long long off;  // LINES: element offset of the first line
     int lines;      // LINES: lines in this item
-    int pad;
+    int grp;        // queue kernel: TMA group of a COLS / ROWS item (-1: 16-byte copies)
 };
 
 struct FsqXform {
@@ -80,6 +80,10 @@ inline int fsq_cols_items(int logn) {
     fsq_split(logn, &n1, &n2);
     return n2 / (FSQ_POINTS / n1);
 }
+__host__ __device__ inline int fsq_cols_items_dev(int logn) {
+    const int n1 = 1 << (logn / 2), n2 = 1 << (logn - logn / 2);
+    return n2 / (FSQ_POINTS / n1);
+}
 inline int fsq_rows_items(int logn) {
     int n1, n2;
     fsq_split(logn, &n1, &n2);
@@ -96,10 +100,41 @@ struct FsqMaps {
     CUtensorMap st;
 };
 
+// ---- one persistent launch over a device-side descriptor queue -------------
+//
+// Mixed sizes: every item of a batch (COLS of every four-step transform,
+// then LINES, then ROWS) in one array; CTAs draw items by atomic ticket.  A
+// ROWS item waits (bounded) until the COLS items of its transform have all
+// been counted done; tickets are drawn in array order, so every COLS item is
+// held by some CTA before any ROWS item is drawn, and a CTA publishes its
+// finished COLS item before it ever waits.  Four-step transforms of one TMA
+// size class that sit back to back form a group whose tiles move by TMA.
+constexpr int FSQ_MAX_GROUPS = 8;
+struct FsqGroup {
+    long long off;      // element offset of the group's first transform in in / out
+    long long scratch;  // element offset of its first intermediate
+    int logn;
+    int pad;
+};
+struct FsqGroupMaps {
+    CUtensorMap ld;    // input as rows of n2 (COLS load)
+    CUtensorMap stc;   // intermediate as rows of n2 (COLS store)
+    CUtensorMap str;   // output as rows of n1 (ROWS store)
+};
+struct FsqQueueArgs {
+    FsqArgs a;        // in, out, scratch, items, xf, nitems, tabs, adjoint
+    int* counters;    // [0] next ticket, [1 + x] COLS items done of transform x
+    int ngroups;
+    FsqGroup groups[FSQ_MAX_GROUPS];
+    FsqGroupMaps maps[FSQ_MAX_GROUPS];
+};
+
 cudaError_t fsq_prepare();
 // Launches one pass over a.nitems items on `s`.
 cudaError_t fsq_launch(const FsqArgs& a, bool inverse, int sms, cudaStream_t s);
 // The same uniform pass with TMA tiles (four-step n = 2^16 .. 2^20 only).
 cudaError_t fsq_launch_tma(const FsqArgs& a, const FsqMaps& m, bool inverse, int sms, int* dev_err, cudaStream_t s);
+// The whole queue in one launch; q.counters must be zero when it starts.
+cudaError_t fsq_launch_queue(const FsqQueueArgs& q, bool inverse, int sms, int* dev_err, cudaStream_t s);
 
 }  // namespace mfft

@@ -1,19 +1,21 @@
-// multi.cu -- FFTs of mixed sizes in one CUDA graph of at most two launches
-// of the item kernel (fsqueue.h/.cu).
+// multi.cu -- FFTs of mixed sizes in ONE persistent launch of the queue
+// kernel (fsqueue.h/.cu), driven by a device-side descriptor queue.
 //
 // No reference counterpart (MetalFFT.forward(batch:) takes one size; its
 // four-step path even loops one command buffer per element,
 // Sources/MetalFFT/FFT/MetalFFT.swift:198-202).  Here the host turns the size
-// classes into two item lists of 4096 points per item:
-//   pass 0   the COLS items of every four-step transform (n >= 8192), then
-//            the whole-line items (n <= 4096, 4096/n lines each), which fill
-//            the tail of the launch;
-//   pass 1   the ROWS items of every four-step transform (absent when there
-//            is none).
-// Four-step classes of 2^16 .. 2^20 points skip the lists: their transforms
-// are contiguous, so each class runs the uniform passes whose tiles move by
-// TMA (fourstep.cu), its column pass after list pass 0 and its row pass after
-// list pass 1.
+// classes once into one array of 4096-point work items, in ticket order:
+//   COLS  the column items of every four-step transform (n >= 8192),
+//         transform by transform;
+//   LINES the whole-line items (n <= 4096, 4096/n lines each);
+//   ROWS  the row items of every four-step transform, in the same order.
+// Each call zeroes the queue's counters and launches the kernel once: CTAs
+// draw items by atomic ticket; a ROWS item starts when its transform's COLS
+// items have been counted done (bounded wait), and the LINES items between
+// the two phases keep the CTAs busy while the last columns finish.
+// Four-step classes of 2^16 .. 2^20 points (up to FSQ_MAX_GROUPS of them) move
+// their tiles by TMA inside the same launch: their transforms sit back to
+// back, so one set of tensor maps per class covers them.
 #include <algorithm>
 #include <vector>
 
@@ -26,13 +28,14 @@ using namespace mfft;
 struct mfft_multi {
     mfft_ctx* ctx = nullptr;
     int64_t points = 0;
-    FsqItem* d_items = nullptr;  // pass 0 items, then pass 1 items
+    FsqItem* d_items = nullptr;  // the queue, in ticket order
     FsqXform* d_xf = nullptr;
+    int* d_counters = nullptr;   // ticket + one COLS count per four-step transform
     float2* scratch = nullptr;   // every four-step intermediate
-    int nitems0 = 0, nitems1 = 0;
+    int nitems = 0, nxf = 0;
     FsqTables tabs{};
     std::vector<float2*> tables;  // owned four-step W_n tables
-    struct Group {                // a four-step class run by the TMA passes
+    struct Group {                // a four-step class whose tiles move by TMA
         int64_t offset, count;
         int logn;
         long long scratch;
@@ -45,6 +48,7 @@ extern "C" int mfft_multi_destroy(mfft_multi* m) {
     DeviceGuard g(m->ctx->device);
     cudaFree(m->d_items);
     cudaFree(m->d_xf);
+    cudaFree(m->d_counters);
     cudaFree(m->scratch);
     for (float2* t : m->tables) cudaFree(t);
     delete m;
@@ -99,6 +103,7 @@ extern "C" int mfft_multi_create(mfft_ctx* ctx, const mfft_multi_desc* descs, in
                 it.logn = logn;
                 it.off = d.offset + l * d.n;
                 it.lines = (int)std::min<int64_t>(per, d.count - l);
+                it.grp = -1;
                 lines.push_back(it);
             }
             continue;
@@ -111,10 +116,10 @@ extern "C" int mfft_multi_create(mfft_ctx* ctx, const mfft_multi_desc* descs, in
             m->tabs.fine[logn - 13] = t;
             m->tabs.coarse[logn - 13] = t + 1024;
         }
-        if (fsq_tma_size(logn)) {
+        int grp = -1;
+        if (fsq_tma_size(logn) && (int)m->groups.size() < FSQ_MAX_GROUPS) {
+            grp = (int)m->groups.size();
             m->groups.push_back(mfft_multi::Group{d.offset, d.count, logn, scratch_pts});
-            scratch_pts += d.n * d.count;
-            continue;
         }
         const int nc = fsq_cols_items(logn), nr = fsq_rows_items(logn);
         for (int64_t j = 0; j < d.count; ++j) {
@@ -125,8 +130,8 @@ extern "C" int mfft_multi_create(mfft_ctx* ctx, const mfft_multi_desc* descs, in
             x.logn = logn;
             scratch_pts += d.n;
             xfs.push_back(x);
-            for (int c = 0; c < nc; ++c) cols.push_back(FsqItem{FSQ_COLS, logn, c, id, 0, 0, 0});
-            for (int r = 0; r < nr; ++r) rows.push_back(FsqItem{FSQ_ROWS, logn, r, id, 0, 0, 0});
+            for (int c = 0; c < nc; ++c) cols.push_back(FsqItem{FSQ_COLS, logn, c, id, 0, 0, grp});
+            for (int r = 0; r < nr; ++r) rows.push_back(FsqItem{FSQ_ROWS, logn, r, id, 0, 0, grp});
         }
     }
     if (st) {
@@ -135,17 +140,17 @@ extern "C" int mfft_multi_create(mfft_ctx* ctx, const mfft_multi_desc* descs, in
     }
     std::vector<FsqItem> q = cols;
     q.insert(q.end(), lines.begin(), lines.end());
-    const size_t n0 = q.size();
     q.insert(q.end(), rows.begin(), rows.end());
-    if (n0 > 0x7fffffff || rows.size() > 0x7fffffff) {
+    if (q.size() > 0x3fffffff || xfs.size() > 0x3fffffff) {
         mfft_multi_destroy(m);
         return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "too many work items");
     }
-    m->nitems0 = (int)n0;
-    m->nitems1 = (int)rows.size();
+    m->nitems = (int)q.size();
+    m->nxf = (int)xfs.size();
     cudaError_t e = cudaSuccess;
     if (!q.empty()) e = cudaMalloc(&m->d_items, sizeof(FsqItem) * q.size());
     if (e == cudaSuccess && !xfs.empty()) e = cudaMalloc(&m->d_xf, sizeof(FsqXform) * xfs.size());
+    if (e == cudaSuccess) e = cudaMalloc(&m->d_counters, sizeof(int) * (1 + xfs.size()));
     if (e == cudaSuccess && scratch_pts) e = cudaMalloc(&m->scratch, sizeof(float2) * scratch_pts);
     if (e == cudaSuccess && !q.empty())
         e = cudaMemcpy(m->d_items, q.data(), sizeof(FsqItem) * q.size(), cudaMemcpyHostToDevice);
@@ -160,34 +165,36 @@ extern "C" int mfft_multi_create(mfft_ctx* ctx, const mfft_multi_desc* descs, in
     return MFFT_SUCCESS;
 }
 
+// One memset of the queue counters and one launch.  The tensor maps of the
+// TMA classes depend on the buffers, so they are encoded per call (host work,
+// baked into a captured graph like any kernel argument).
 static int multi_device(mfft_multi* m, const float2* in, float2* out, int direction, cudaStream_t s) {
-    FsqArgs a{};
-    a.in = in;
-    a.out = out;
-    a.scratch = m->scratch;
-    a.items = m->d_items;
-    a.xf = m->d_xf;
-    a.nitems = m->nitems0;
-    a.tabs = m->tabs;
-    const bool inv = direction == MFFT_INVERSE;
-    cudaError_t e = fsq_launch(a, inv, m->ctx->sms, s);
+    if (m->nitems == 0) return MFFT_SUCCESS;
+    FsqQueueArgs q{};
+    q.a.in = in;
+    q.a.out = out;
+    q.a.scratch = m->scratch;
+    q.a.items = m->d_items;
+    q.a.xf = m->d_xf;
+    q.a.nitems = m->nitems;
+    q.a.tabs = m->tabs;
+    q.counters = m->d_counters;
+    q.ngroups = (int)m->groups.size();
+    for (int gi = 0; gi < q.ngroups; ++gi) {
+        const auto& g = m->groups[gi];
+        int n1, n2;
+        fsq_split(g.logn, &n1, &n2);
+        const int C = FSQ_POINTS / n1, RW = FSQ_POINTS / n2;
+        q.groups[gi] = FsqGroup{g.offset, g.scratch, g.logn, 0};
+        FsqGroupMaps& mp = q.maps[gi];
+        if (!encode_rows(&mp.ld, in + g.offset, (uint64_t)g.count * n1, n2, C) ||
+            !encode_rows(&mp.stc, m->scratch + g.scratch, (uint64_t)g.count * n1, n2, C) ||
+            !encode_rows(&mp.str, out + g.offset, (uint64_t)g.count * n2, n1, RW))
+            return set_error(MFFT_ERR_LIBRARY_BUILD, -1, -1, -1, "mixed-size tensor maps could not be encoded");
+    }
+    cudaError_t e = cudaMemsetAsync(m->d_counters, 0, sizeof(int) * (1 + m->nxf), s);
+    if (e == cudaSuccess) e = fsq_launch_queue(q, direction == MFFT_INVERSE, m->ctx->sms, m->ctx->dev_err, s);
     if (e != cudaSuccess) return cuda_error(e, "mixed-size launch");
-    for (const auto& g : m->groups) {
-        int st = fourstep_tma_pass(FSQ_COLS, m->tabs, in + g.offset, out + g.offset, m->scratch + g.scratch, g.count,
-                                   g.logn, inv, m->ctx, s);
-        if (st) return st;
-    }
-    if (m->nitems1) {
-        a.items = m->d_items + m->nitems0;
-        a.nitems = m->nitems1;
-        e = fsq_launch(a, inv, m->ctx->sms, s);
-        if (e != cudaSuccess) return cuda_error(e, "mixed-size launch");
-    }
-    for (const auto& g : m->groups) {
-        int st = fourstep_tma_pass(FSQ_ROWS, m->tabs, in + g.offset, out + g.offset, m->scratch + g.scratch, g.count,
-                                   g.logn, inv, m->ctx, s);
-        if (st) return st;
-    }
     return MFFT_SUCCESS;
 }
 
@@ -195,9 +202,9 @@ extern "C" int mfft_multi_exec(mfft_multi* m, const void* in, void* out, int dir
     if (!m) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "multi is NULL");
     int st = check_exec_args(in, out, m->points, direction, flags);
     if (st) return st;
-    // in == out is safe: the row pass, which writes the four-step outputs,
-    // starts after the column pass has read every input; LINES items read
-    // and write the same elements.
+    // in == out is safe: a transform's ROWS items, which write its output,
+    // start only after all of its COLS items have read its input; LINES items
+    // read and write the same elements.
     DeviceGuard g(m->ctx->device);
     if (flags == MFFT_DEVICE_MEMORY)
         return multi_device(m, (const float2*)in, (float2*)out, direction, (cudaStream_t)stream);

@@ -28,10 +28,10 @@
 //   BF16:       one product of bf16 operands.
 //
 // One persistent CTA per SM, warp-specialised, every hand-off an mbarrier:
-//   converter warps 0-3   load a line (streaming loads, the line two ahead
-//                         prefetched into L2), find its power-of-two scale,
-//                         write the stage-1 operand (hi/lo) into one of
-//                         three operand buffers
+//   converter warps 0-3   load a line (coalesced 16-byte streaming loads,
+//                         the line two ahead prefetched into L2), find its
+//                         power-of-two scale, write the stage-1 operand
+//                         (hi/lo) into one of three operand buffers
 //   MMA warp 12 (1 thread) stage-1 products of line i, then stage-2 products
 //                         of line i-1; the DFT-64 operand G lives in tensor
 //                         memory (the A operand), so the tensor core reads
@@ -40,7 +40,9 @@
 //                         W4096^(n2 k1) 2^-10 (one table, the scale change
 //                         between the stages folded in) -> stage-2 operand in
 //                         the same operand buffer
-//   epilogue-2 warps 8-11 stage-2 accumulators -> unscaled X, streamed out
+//   epilogue-2 warps 8-11 stage-2 accumulators -> unscaled X in a shared-
+//                         memory tile (128-byte swizzle), written out by TMA
+//                         tensor stores: four boxes of 16 columns x 64 rows
 // Two accumulator slots per stage (TMEM columns 128-383; G in 0-127), three
 // operand buffers: while the tensor core runs one line, the converter, the
 // two epilogues and the loads work on up to four others.  Every wait is
@@ -144,6 +146,27 @@ __device__ __forceinline__ void store_chunk_b(uint8_t* b, uint32_t off, const fl
     }
 }
 
+// 2 FP32 values -> 4 bytes of the operand (hi/lo planes or bf16)
+template <bool SPLIT>
+__device__ __forceinline__ void store_pair_b(uint8_t* b, uint32_t off, float x0, float x1) {
+    if constexpr (SPLIT) {
+        const __half2 h = __floats2half2_rn(x0, x1);
+        const float2 hf = __half22float2(h);
+        const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+        *reinterpret_cast<__half2*>(b + off) = h;
+        *reinterpret_cast<__half2*>(b + 16384 + off) = l;
+    } else {
+        *reinterpret_cast<__nv_bfloat162*>(b + off) = __floats2bfloat162_rn(x0, x1);
+    }
+}
+
+__device__ __forceinline__ void tma_store_2d_tc(const CUtensorMap* map, int x, int y, const void* src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(smem_u32(src))
+                 : "memory");
+}
+
 // bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned) into L2
 __device__ __forceinline__ void prefetch_l2(const void* g, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g), "r"(bytes) : "memory");
@@ -158,7 +181,9 @@ constexpr int TW_ND = 2;     // accumulator slots per stage
 constexpr int TW_NS1 = 8;    // line-scale ring (the converter runs at most 5 lines ahead of epilogue 2)
 constexpr uint32_t TW_OPB = 32768;                       // one operand buffer: hi 16 KB + lo 16 KB
 constexpr uint32_t TW_TAB = TW_NOP * TW_OPB;             // twiddle table: 4096 float2 = 32 KB
-constexpr uint32_t TW_SMEM = TW_TAB + 32768 + 1024;      // + alignment slack
+constexpr uint32_t TW_OUT = TW_TAB + 32768;              // two output tiles of 32 KB (4 boxes of 8 KB)
+constexpr uint32_t TW_SMEM = TW_OUT + 2 * 32768 + 1024;  // + alignment slack
+constexpr long long TW_MAX_LINES = 1LL << 24;            // per launch: output row 64*line fits in 31 bits
 constexpr uint32_t TW_GCOL = 0, TW_D1COL = 128, TW_D2COL = 256;  // TMEM columns
 constexpr int TW_BAR_CONV = 1, TW_BAR_EPI1 = 2, TW_BAR_EPI2 = 3;  // named barriers (0 is __syncthreads)
 
@@ -190,7 +215,7 @@ __device__ __forceinline__ void pair_half(const float (&v)[32], int bsel, float 
 
 template <bool SPLIT, bool INV>
 __global__ void __launch_bounds__(TW_THREADS, 1)
-    k_fft4096_tcw(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
+    k_fft4096_tcw(const float2* __restrict__ in, long long batch, const __grid_constant__ CUtensorMap omap,
                   const uint4* __restrict__ gplain, const float2* __restrict__ tw, int* dev_err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t op_full1[TW_NOP], op_full2[TW_NOP], op_empty[TW_NOP];
@@ -281,24 +306,23 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
             const long long f = blockIdx.x + i * G;
             const int o = (int)(i % TW_NOP);
             if (ctid == 0 && i + 2 < nlines) prefetch_l2(in + (size_t)(f + 2 * G) * TC_N, TC_N * sizeof(float2));
+            // float4 q = ctid + 128 r holds x[2q], x[2q+1]: n1 = warp + 4 r, n2 = 2 lane (+1)
             float4 cur[16];
-            const float4* src = reinterpret_cast<const float4*>(in + (size_t)f * TC_N);
+            const float4* src = reinterpret_cast<const float4*>(in + (size_t)f * TC_N) + ctid;
 #pragma unroll
-            for (int it = 0; it < 4; ++it)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) cur[4 * it + j] = __ldcs(src + 4 * (ctid + 128 * it) + j);
+            for (int r = 0; r < 16; ++r) cur[r] = __ldcs(src + 128 * r);
             if constexpr (INV) {
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    cur[q].y = -cur[q].y;
-                    cur[q].w = -cur[q].w;
+                for (int r = 0; r < 16; ++r) {
+                    cur[r].y = -cur[r].y;
+                    cur[r].w = -cur[r].w;
                 }
             }
             if constexpr (SPLIT) {
                 float mx = 0.f;
 #pragma unroll
-                for (int q = 0; q < 16; ++q)
-                    mx = fmaxf(mx, fmaxf(fmaxf(fabsf(cur[q].x), fabsf(cur[q].y)), fmaxf(fabsf(cur[q].z), fabsf(cur[q].w))));
+                for (int r = 0; r < 16; ++r)
+                    mx = fmaxf(mx, fmaxf(fmaxf(fabsf(cur[r].x), fabsf(cur[r].y)), fmaxf(fabsf(cur[r].z), fabsf(cur[r].w))));
 #pragma unroll
                 for (int sh = 16; sh > 0; sh >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, sh));
                 if (lane == 0) red[i & 1][warp] = mx;
@@ -310,21 +334,13 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
             float s1 = 1.f;
             if constexpr (SPLIT) s1 = line_scale(fmaxf(fmaxf(red[i & 1][0], red[i & 1][1]), fmaxf(red[i & 1][2], red[i & 1][3])));
             uint8_t* bp = smem + (uint32_t)o * TW_OPB;
+            // a warp writes 64 halves (one 128-byte row) per row: no bank conflicts
 #pragma unroll
-            for (int it = 0; it < 4; ++it) {
-                const int item = ctid + 128 * it;  // (n1, c): n2 = 8c .. 8c+7
-                const int n1 = item >> 3, c = item & 7;
-                float re[8], im[8];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const float4 v = cur[4 * it + j];
-                    re[2 * j] = v.x * s1;
-                    im[2 * j] = v.y * s1;
-                    re[2 * j + 1] = v.z * s1;
-                    im[2 * j + 1] = v.w * s1;
-                }
-                store_chunk_b<SPLIT>(bp, mnmaj_off(8 * c, 2 * n1), re);
-                store_chunk_b<SPLIT>(bp, mnmaj_off(8 * c, 2 * n1 + 1), im);
+            for (int r = 0; r < 16; ++r) {
+                const int n1 = warp + 4 * r;
+                const float4 v = cur[r];
+                store_pair_b<SPLIT>(bp, mnmaj_off(2 * lane, 2 * n1), v.x * s1, v.z * s1);
+                store_pair_b<SPLIT>(bp, mnmaj_off(2 * lane, 2 * n1 + 1), v.y * s1, v.w * s1);
             }
             if (ctid == 0) {
                 s1ring[i % TW_NS1] = s1;
@@ -375,6 +391,9 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
         }
     } else if (warp < TW_EPI2 + 4) {
         // ---------------- epilogue 2: X out ----------------
+        // tile of line i: buffer i & 1, box bx (columns k1 = 16 bx .. 16 bx + 15)
+        // of 64 rows k2 x 128 bytes, 16-byte chunk c of row k2 at c ^ (k2 % 8)
+        // (the tensor map's 128-byte swizzle)
         const int q = warp & 3, m = 32 * q + lane;
         const int k2 = m >> 1, bsel = m & 1;
         const uint32_t lane_off = (uint32_t)(32 * q) << 16;
@@ -382,10 +401,14 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
         for (long long i = 0; i < nlines; ++i) {
             const long long f = blockIdx.x + i * G;
             const int d = (int)(i % TW_ND);
+            uint8_t* ot = smem + TW_OUT + (uint32_t)(i & 1) * 32768;
             bool ok = true;
-            if (m == 0)
+            if (m == 0) {
                 ok = wait_or_abort(&d2_full[d], (uint32_t)((i / TW_ND) & 1), abort_sh) &&
                      wait_or_abort(&s1_full[i % TW_NS1], (uint32_t)((i / TW_NS1) & 1), abort_sh);
+                // the tile written two lines ago has been read by its tensor stores
+                asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+            }
             if (bar_or(TW_BAR_EPI2, 128, !ok)) break;
             tc::fence_after_sync();
             // X = D2 / (16 s2), s2 = s1 / 64 (split); X = D2 (bf16)
@@ -401,8 +424,7 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
             for (int h = 0; h < 2; ++h) {
                 float2 z[16];
                 pair_half(h ? v1 : v0, bsel, sc, z);
-                const int k1_0 = 32 * h + 16 * bsel;
-                float4* dst = reinterpret_cast<float4*>(out + (size_t)f * TC_N + TC_R * k2 + k1_0);
+                uint8_t* row = ot + (uint32_t)(2 * h + bsel) * 8192 + (uint32_t)k2 * 128;
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     float4 o4 = make_float4(z[2 * j].x, z[2 * j].y, z[2 * j + 1].x, z[2 * j + 1].y);
@@ -410,10 +432,18 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
                         o4.y = -o4.y;
                         o4.w = -o4.w;
                     }
-                    __stcs(dst + j, o4);
+                    *reinterpret_cast<float4*>(row + ((j ^ (k2 & 7)) << 4)) = o4;
                 }
             }
+            fence_proxy_async_smem();  // the tile's generic writes before the tensor stores read it
+            asm volatile("bar.sync %0, %1;" ::"r"(TW_BAR_EPI2), "r"(128) : "memory");
+            if (m == 0) {
+#pragma unroll
+                for (int bx = 0; bx < 4; ++bx) tma_store_2d_tc(&omap, 32 * bx, (int)(64 * f), ot + bx * 8192);
+                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            }
         }
+        if (m == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     } else if (warp == TW_MMA && lane == 0) {
         // ---------------- MMA issue: stage 1 of line i, stage 2 of line i - 1 ----------------
         constexpr int NPROD = SPLIT ? 3 : 1;
@@ -485,17 +515,25 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
     }
 }
 
+// Launches over at most TW_MAX_LINES lines each; the output goes through a
+// tensor map of the chunk's lines as 64-row x 512-byte blocks.
 template <bool SPLIT, bool INV>
 cudaError_t launch_tcw(const float2* in, float2* out, long long batch, const uint4* gplain, const float2* tw,
                        int* dev_err, int sms, cudaStream_t s) {
     cudaError_t e = cudaFuncSetAttribute(k_fft4096_tcw<SPLIT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          TW_SMEM);
     if (e != cudaSuccess) return e;
-    long long blocks = batch;
-    if (blocks > sms) blocks = sms;
-    if (blocks <= 0) return cudaSuccess;
-    k_fft4096_tcw<SPLIT, INV><<<(unsigned)blocks, TW_THREADS, TW_SMEM, s>>>(in, out, batch, gplain, tw, dev_err);
-    return cudaGetLastError();
+    for (long long b0 = 0; b0 < batch; b0 += TW_MAX_LINES) {
+        const long long nb = batch - b0 < TW_MAX_LINES ? batch - b0 : TW_MAX_LINES;
+        CUtensorMap omap;
+        if (!encode_rows(&omap, out + b0 * TC_N, (uint64_t)nb * TC_R, TC_R, 16, TC_R)) return cudaErrorInvalidValue;
+        const long long blocks = nb < sms ? nb : sms;
+        k_fft4096_tcw<SPLIT, INV><<<(unsigned)blocks, TW_THREADS, TW_SMEM, s>>>(in + b0 * TC_N, nb, omap, gplain, tw,
+                                                                                 dev_err);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace

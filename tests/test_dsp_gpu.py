@@ -266,6 +266,14 @@ def test_mixed_small_set(M):
     _check_mixed(M, classes, seed=32, inverse=True)
 
 
+def test_mixed_more_tma_classes_than_groups(M):
+    # ten 2^16 classes: the first eight move their tiles by TMA inside the
+    # queue launch, the last two take the 16-byte-copy items of the same kernel
+    classes = [(1 << 16, 1)] * 10 + [(64, 5), (1 << 15, 1)]
+    _check_mixed(M, classes, seed=34)
+    _check_mixed(M, classes, seed=35, inverse=True)
+
+
 def test_mixed_config2_full(M):
     from metalfft_b200 import workloads
     classes = workloads.mixed_size_classes()
@@ -285,8 +293,8 @@ def test_mixed_host_arrays(M):
 
 
 def test_mixed_in_place_matches_out_of_place(M):
-    # in == out: the row passes, which write the four-step outputs, run after
-    # every column pass has read its input (item lists and TMA classes alike)
+    # in == out: a transform's row items, which write its output, start after
+    # all of its column items have read its input (TMA classes alike)
     import torch
     classes = [(256, 7), (4096, 3), (8192, 2), (1 << 15, 1), (1 << 16, 2), (1 << 18, 1), (1 << 20, 2)]
     mb = M.MixedBatch(classes)
@@ -300,9 +308,9 @@ def test_mixed_in_place_matches_out_of_place(M):
 
 
 def test_mixed_graph_replay_matches_exec(M):
-    # config 2 runs as one CUDA graph per step: the captured launches (the
-    # item lists and the TMA passes, tensor maps passed by value) replay to
-    # the same bits as a direct call, twice in a row
+    # config 2 runs as one CUDA graph per step: the captured counter reset and
+    # queue launch (tensor maps passed by value) replay to the same bits as a
+    # direct call, twice in a row
     import torch
     classes = [(64, 9), (2048, 3), (16384, 2), (1 << 16, 1), (1 << 20, 2)]
     mb = M.MixedBatch(classes)
