@@ -450,19 +450,50 @@ __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
     return v;
 }
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+__device__ __forceinline__ int ld_relaxed_gpu(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// An item with its transform's offsets, read from the queue one ticket ahead
+// (a 48-byte cp.async into shared memory) and handed to every thread there.
+typedef FsqItem QDesc;
+
+__device__ __forceinline__ Work q_work(const QDesc& d) {
+    Work w;
+    w.kind = d.kind;
+    w.logn = d.logn;
+    w.index = d.index;
+    w.lines = d.lines;
+    w.off = d.kind == FSQ_LINES ? d.off : d.xoff;
+    w.scratch = d.kind == FSQ_LINES ? 0 : d.xscratch;
+    return w;
+}
+
+// thread 0: queue entry p -> dst (shared memory), as one cp.async group
+__device__ __forceinline__ void q_prefetch_desc(const FsqQueueArgs& q, int p, QDesc* dst) {
+    const float2* src = reinterpret_cast<const float2*>(q.a.items + p);
+    float2* d = reinterpret_cast<float2*>(dst);
+#pragma unroll
+    for (int k = 0; k < (int)(sizeof(QDesc) / 16); ++k) cp_async16(d + 2 * k, src + 2 * k);
+    cp_async_commit();
+}
 
 // transform index of a TMA item inside its group
-__device__ __forceinline__ long long q_group_index(const FsqQueueArgs& q, const FsqItem& it) {
-    return (q.a.xf[it.xform].off - q.groups[it.grp].off) >> it.logn;
+__device__ __forceinline__ long long q_group_index(const FsqQueueArgs& q, const QDesc& d) {
+    return (d.xoff - q.groups[d.grp].off) >> d.logn;
 }
 
 // every thread: item `p`'s data into stage `st`, completion on `bar`
 // (256 arrivals: cp.async copies of every thread, or thread 0's bulk copies
 // counted in bytes plus 255 plain arrivals)
-__device__ __forceinline__ void q_issue(const FsqQueueArgs& q, int p, float2* st, uint64_t* bar, uint64_t pol) {
-    const FsqItem it = q.a.items[p];
+__device__ __forceinline__ void q_issue(const FsqQueueArgs& q, const QDesc& d, float2* st, uint64_t* bar,
+                                        uint64_t pol) {
+    const FsqItem& it = d;
     if (it.grp < 0) {
-        issue(q.a, get_work(q.a, p), st, pol);
+        issue(q.a, q_work(d), st, pol);
         cp_async_mbar_arrive(bar);
         return;
     }
@@ -473,7 +504,7 @@ __device__ __forceinline__ void q_issue(const FsqQueueArgs& q, int p, float2* st
     const FsqGroupMaps& m = q.maps[it.grp];
     const int l1 = it.logn / 2, l2 = it.logn - l1;
     mbar_arrive_expect_tx(bar, FSQ_POINTS * (uint32_t)sizeof(float2));
-    const long long j = q_group_index(q, it);
+    const long long j = q_group_index(q, d);
     if (it.kind == FSQ_COLS) {
         const int lc = ilog2c(FSQ_POINTS) - l1;
         const int x = (it.index << lc) * 2;  // floats
@@ -484,17 +515,17 @@ __device__ __forceinline__ void q_issue(const FsqQueueArgs& q, int p, float2* st
         // the intermediate was written by other CTAs (generic and async proxies)
         fence_proxy_async_global();
         const int lr = ilog2c(FSQ_POINTS) - l2;
-        const FsqXform x = q.a.xf[it.xform];
-        bulk_g2s(st, q.a.scratch + x.scratch + ((long long)it.index << (lr + l2)), FSQ_POINTS * (uint32_t)sizeof(float2),
-                 bar);
+        bulk_g2s(st, q.a.scratch + d.xscratch + ((long long)it.index << (lr + l2)),
+                 FSQ_POINTS * (uint32_t)sizeof(float2), bar);
     }
 }
 
 // thread 0: the finished tile of TMA item `it` from stage `st`
-__device__ __forceinline__ void q_tma_store(const FsqQueueArgs& q, const FsqItem& it, const float2* st) {
+__device__ __forceinline__ void q_tma_store(const FsqQueueArgs& q, const QDesc& d, const float2* st) {
+    const FsqItem& it = d;
     const FsqGroupMaps& m = q.maps[it.grp];
     const int l1 = it.logn / 2, l2 = it.logn - l1;
-    const long long j = q_group_index(q, it);
+    const long long j = q_group_index(q, d);
     if (it.kind == FSQ_COLS) {
         const int lc = ilog2c(FSQ_POINTS) - l1, C = 1 << lc;
         const int x = (it.index << lc) * 2;
@@ -514,8 +545,7 @@ __device__ __forceinline__ int q_cols_needed(int logn) { return fsq_cols_items_d
 
 // thread 0: for a ROWS item, waits (bounded) until every COLS item of its
 // transform is counted done; other items need nothing
-__device__ __forceinline__ bool q_wait_cols(const FsqQueueArgs& q, int p) {
-    const FsqItem it = q.a.items[p];
+__device__ __forceinline__ bool q_wait_cols(const FsqQueueArgs& q, const QDesc& it) {
     if (it.kind != FSQ_ROWS) return true;
     const int need = q_cols_needed(it.logn);
     if (ld_acquire_gpu(q.counters + 1 + it.xform) >= need) return true;
@@ -525,37 +555,84 @@ __device__ __forceinline__ bool q_wait_cols(const FsqQueueArgs& q, int p) {
     return true;
 }
 
-// thread 0: publish a finished COLS item of transform x (its tile stores
-// done and visible GPU-wide before the count that ROWS items acquire)
-__device__ __forceinline__ void q_publish(const FsqQueueArgs& q, int x, bool tma) {
-    if (x < 0) return;
-    if (tma) {
-        bulk_wait_all();
+__device__ __forceinline__ void red_release_add(int* p, int v) {
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void bulk_wait_all_but_one() { asm volatile("cp.async.bulk.wait_group 1;" ::: "memory"); }
+
+// A finished item as thread 0 remembers it until it is counted: x = its
+// transform when it is a COLS item (-1 otherwise), tma = it committed a bulk
+// store group (TMA items do).
+struct QDone {
+    int x;
+    bool tma;
+};
+
+// thread 0: count finished COLS item d; `newer` = a bulk group committed after
+// d's own may still be pending.  The count is a release: d's tile stores
+// (made by every thread before a CTA barrier thread 0 has passed, or by its
+// bulk store, waited for here) are visible GPU-wide before ROWS items acquire
+// the count.
+__device__ __forceinline__ void q_count(const FsqQueueArgs& q, const QDone& d, bool newer) {
+    if (d.x < 0) return;
+    if (d.tma) {
+        if (newer) bulk_wait_all_but_one();
+        else bulk_wait_all();
         fence_proxy_async_global();
     }
-    __threadfence();
-    atomicAdd(q.counters + 1 + x, 1);
+    red_release_add(q.counters + 1 + d.x, 1);
 }
 
+// Tickets are drawn one item ahead (the atomic's latency hides behind an
+// item's work), and a finished COLS item is counted two items later, when its
+// stores have long landed, so no thread stalls on either in steady state.
+// A CTA counts everything it holds before it waits for a ROWS item's
+// columns, so no wait depends on its own work.
 template <bool INV>
 __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
     k_fsq_queue(const __grid_constant__ FsqQueueArgs q, int* dev_err) {
     extern __shared__ __align__(1024) unsigned char fsq_raw[];
     __shared__ __align__(8) uint64_t bar[2];
+    __shared__ QDesc sh_desc[2];  // the item of each stage
+    __shared__ QDesc sh_pre[2];   // descriptors prefetched for the next ticket
     __shared__ int sh_next, sh_ready;
     float2* smem = reinterpret_cast<float2*>(fsq_raw + ((1024u - (smem_u32(fsq_raw) & 1023u)) & 1023u));
     const int n = q.a.nitems;
     const uint64_t pol = policy_evict_first();
     // every item, the first included, is drawn by ticket: a CTA that draws a
     // ROWS item knows that running CTAs hold all of its transform's COLS items
+    // Thread 0 works three tickets ahead of the item it issues: t1 (its
+    // descriptor in shared memory, its readiness read one iteration ago), t2
+    // (descriptor landed this iteration, readiness read now), t3 (the atomic
+    // draw, consumed next iteration).  A ROWS item's column count is read
+    // relaxed one iteration early; a ROWS item is issued after an acquire fence
+    // once that count is complete, and re-read (and waited for) only when the
+    // early read fell short.
     bool first_ok = true;
+    int t1 = n, t2 = n, t3 = n;
+    int r1 = 1;     // thread 0: t1's column count was complete when read (or t1 is not a ROWS item)
+    int pslot = 0;  // thread 0: sh_pre slot holding t1's descriptor (t2's is the other one)
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], FSQ_THREADS);
         mbar_init(&bar[1], FSQ_THREADS);
         fence_proxy_async_smem();
         const int c = atomicAdd(q.counters, 1);
         sh_next = c;
-        if (c < n) first_ok = q_wait_cols(q, c);
+        if (c < n) {
+            const QDesc dc = q.a.items[c];
+            t1 = atomicAdd(q.counters, 1);
+            if (t1 < n) {
+                t2 = atomicAdd(q.counters, 1);
+                if (t2 < n) t3 = atomicAdd(q.counters, 1);
+                const QDesc d1v = q.a.items[t1];
+                sh_pre[0] = d1v;
+                r1 = d1v.kind != FSQ_ROWS || ld_relaxed_gpu(q.counters + 1 + d1v.xform) >= q_cols_needed(d1v.logn);
+            }
+            sh_desc[0] = dc;
+            first_ok = q_wait_cols(q, dc);
+        }
+        if (t2 < n) q_prefetch_desc(q, t2, &sh_pre[1]);
+        else cp_async_commit();
     }
     if (__syncthreads_or(!first_ok)) {
         if (threadIdx.x == 0) report_device_error(dev_err, DEV_ERR_QUEUE_TIMEOUT);
@@ -563,23 +640,43 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
     }
     int cur = sh_next;
     if (cur >= n) return;
-    q_issue(q, cur, smem, &bar[0], pol);
+    q_issue(q, sh_desc[0], smem, &bar[0], pol);
+    if (threadIdx.x == 0) cp_async_commit();  // thread 0's groups: descriptor, data, descriptor, ...
     uint32_t ph[2] = {0u, 0u};
     int s = 0;
-    int pending = -1;  // thread 0: transform of a finished, not yet published COLS item
-    bool pending_tma = false;
+    QDone d1{-1, false}, d2{-1, false};  // thread 0: the previous item, the one before it
     bool failed = false;
     for (;;) {
         if (threadIdx.x == 0) {
-            q_publish(q, pending, pending_tma);
-            pending = -1;
-            const int nx = atomicAdd(q.counters, 1);
+            q_count(q, d2, d1.tma);
+            d2 = d1;
+            d1 = QDone{-1, false};
+            cp_async_wait<1>();  // t2's descriptor (all but the latest group, the data copies)
+            const int nx = t1;
             int ready = 1;
             if (nx < n) {
-                const FsqItem it = q.a.items[nx];
-                if (it.kind == FSQ_ROWS)
-                    ready = ld_acquire_gpu(q.counters + 1 + it.xform) >= q_cols_needed(it.logn);
+                const QDesc& dx = sh_pre[pslot];
+                if (dx.kind == FSQ_ROWS) {
+                    ready = r1 || ld_acquire_gpu(q.counters + 1 + dx.xform) >= q_cols_needed(dx.logn);
+                    if (ready) fence_acq_rel_gpu();  // its columns' stores before this CTA's reads
+                }
+                sh_desc[s ^ 1] = dx;
             }
+            // shift the look-ahead: t2 -> t1 (read its count now), t3 -> t2 (prefetch its descriptor)
+            t1 = t2;
+            r1 = 1;
+            if (t1 < n) {
+                const QDesc& dn = sh_pre[pslot ^ 1];
+                if (dn.kind == FSQ_ROWS) r1 = ld_relaxed_gpu(q.counters + 1 + dn.xform) >= q_cols_needed(dn.logn);
+            }
+            t2 = t3;
+            if (t2 < n) {
+                t3 = atomicAdd(q.counters, 1);
+                q_prefetch_desc(q, t2, &sh_pre[pslot]);
+            } else {
+                cp_async_commit();
+            }
+            pslot ^= 1;
             bulk_wait_read_all();  // the other stage is no longer read by a bulk store
             sh_next = nx;
             sh_ready = ready;
@@ -587,46 +684,45 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
         __syncthreads();
         const int nx = sh_next;
         const bool ready = sh_ready != 0;
-        if (nx < n && ready) q_issue(q, nx, smem + (s ^ 1) * QSTAGE, &bar[s ^ 1], pol);
+        if (nx < n && ready) q_issue(q, sh_desc[s ^ 1], smem + (s ^ 1) * QSTAGE, &bar[s ^ 1], pol);
+        if (threadIdx.x == 0 && (ready || nx >= n)) cp_async_commit();
         const bool landed = mbar_wait(&bar[s], ph[s]);
         ph[s] ^= 1u;
         if (__syncthreads_or(!landed)) {
             failed = true;
             break;
         }
-        const FsqItem it = q.a.items[cur];
-        const Work w = get_work(q.a, cur);
+        const QDesc& dc = sh_desc[s];
+        const Work w = q_work(dc);
         float2* st = smem + s * QSTAGE;
-        if (it.grp >= 0) {
+        if (dc.grp >= 0) {
             compute<INV, true>(q.a, w, st);
             fence_proxy_async_smem();  // the tile's generic writes before the bulk store reads them
             __syncthreads();
-            if (threadIdx.x == 0) q_tma_store(q, it, st);
+            if (threadIdx.x == 0) q_tma_store(q, dc, st);
         } else {
             compute<INV>(q.a, w, st);
-            if (it.kind == FSQ_COLS) __threadfence();  // this thread's tile stores before the count
         }
-        if (threadIdx.x == 0 && it.kind == FSQ_COLS) {
-            pending = it.xform;
-            pending_tma = it.grp >= 0;
-        }
+        if (threadIdx.x == 0) d1 = QDone{dc.kind == FSQ_COLS ? dc.xform : -1, dc.grp >= 0};
         if (nx < n && !ready) {
-            // a ROWS item whose columns are still in flight elsewhere: publish
-            // this CTA's own item first, then wait (bounded)
-            __syncthreads();  // every writer's fence is done
+            // a ROWS item whose columns are still in flight elsewhere: count
+            // this CTA's own items first, then wait (bounded)
+            __syncthreads();  // every thread's tile stores precede the counts
             bool ok = true;
             if (threadIdx.x == 0) {
-                q_publish(q, pending, pending_tma);
-                pending = -1;
-                ok = q_wait_cols(q, nx);
+                q_count(q, d2, d1.tma);
+                q_count(q, d1, false);
+                d1 = d2 = QDone{-1, false};
+                ok = q_wait_cols(q, sh_desc[s ^ 1]);
             }
             if (__syncthreads_or(!ok)) {
                 failed = true;
                 break;
             }
-            q_issue(q, nx, smem + (s ^ 1) * QSTAGE, &bar[s ^ 1], pol);
+            q_issue(q, sh_desc[s ^ 1], smem + (s ^ 1) * QSTAGE, &bar[s ^ 1], pol);
+            if (threadIdx.x == 0) cp_async_commit();
         }
-        __syncthreads();  // every read of stage s is done before it is refilled
+        __syncthreads();  // every read of stage s (and of its descriptor) is done before either is refilled
         if (nx >= n) break;
         cur = nx;
         s ^= 1;
@@ -638,7 +734,8 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
             mbar_wait(&bar[0], ph[0]);
             mbar_wait(&bar[1], ph[1]);
         } else {
-            q_publish(q, pending, pending_tma);
+            q_count(q, d2, d1.tma);
+            q_count(q, d1, false);
         }
         bulk_wait_all();
     }

@@ -29,7 +29,7 @@ constexpr int FSQ_CTAS_PER_SM = 3;
 
 enum : int { FSQ_LINES = 0, FSQ_COLS = 1, FSQ_ROWS = 2 };
 
-struct FsqItem {
+struct alignas(16) FsqItem {
     int kind;
     int logn;       // log2 of the line size (LINES) or of the transform size
     int index;      // COLS: column tile, ROWS: row group
@@ -37,6 +37,8 @@ struct FsqItem {
     long long off;  // LINES: element offset of the first line
     int lines;      // LINES: lines in this item
     int grp;        // queue kernel: TMA group of a COLS / ROWS item (-1: 16-byte copies)
+    long long xoff;      // queue kernel, COLS / ROWS: the transform's offset in in / out
+    long long xscratch;  //   and of its intermediate (the FsqXform, so one read gives both)
 };
 
 struct FsqXform {

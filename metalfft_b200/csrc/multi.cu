@@ -130,8 +130,8 @@ extern "C" int mfft_multi_create(mfft_ctx* ctx, const mfft_multi_desc* descs, in
             x.logn = logn;
             scratch_pts += d.n;
             xfs.push_back(x);
-            for (int c = 0; c < nc; ++c) cols.push_back(FsqItem{FSQ_COLS, logn, c, id, 0, 0, grp});
-            for (int r = 0; r < nr; ++r) rows.push_back(FsqItem{FSQ_ROWS, logn, r, id, 0, 0, grp});
+            for (int c = 0; c < nc; ++c) cols.push_back(FsqItem{FSQ_COLS, logn, c, id, 0, 0, grp, x.off, x.scratch});
+            for (int r = 0; r < nr; ++r) rows.push_back(FsqItem{FSQ_ROWS, logn, r, id, 0, 0, grp, x.off, x.scratch});
         }
     }
     if (st) {

@@ -27,28 +27,32 @@
 //               scales are undone exactly in the epilogues.
 //   BF16:       one product of bf16 operands.
 //
-// One persistent CTA per SM, warp-specialised, every hand-off an mbarrier:
-//   converter warps 0-3   load a line (coalesced 16-byte streaming loads,
-//                         the line two ahead prefetched into L2), find its
-//                         power-of-two scale, write the stage-1 operand
-//                         (hi/lo) into one of three operand buffers
-//   MMA warp 12 (1 thread) stage-1 products of line i, then stage-2 products
-//                         of line i-1; the DFT-64 operand G lives in tensor
+// One persistent CTA per SM, warp-specialised, every hand-off an mbarrier.
+// Lines go in pairs: one MMA of N = 128 covers both lines of a pair (the
+// tensor core's cost per instruction, not its FLOP rate, bounds N = 64).
+//   converter warps 0-7   two groups of four, group g converts line g of each
+//                         pair: coalesced 16-byte streaming loads (the pair
+//                         two ahead prefetched into L2), the line's power-of-
+//                         two scale, its stage-1 operand (hi/lo) into one of
+//                         two 64 KB pair buffers
+//   MMA warp 16 (1 thread) stage-1 products of pair i, then stage-2 products
+//                         of pair i-1; the DFT-64 operand G lives in tensor
 //                         memory (the A operand), so the tensor core reads
-//                         only the line's operand from shared memory
-//   epilogue-1 warps 4-7  stage-1 accumulators (TMEM) -> re/im pairs -> times
+//                         only the operands from shared memory
+//   epilogue-1 warps 8-11 stage-1 accumulators (TMEM) -> re/im pairs -> times
 //                         W4096^(n2 k1) 2^-10 (one table, the scale change
-//                         between the stages folded in) -> stage-2 operand in
-//                         the same operand buffer
-//   epilogue-2 warps 8-11 stage-2 accumulators -> unscaled X in a shared-
-//                         memory tile (128-byte swizzle), written out by TMA
-//                         tensor stores: four boxes of 16 columns x 64 rows
-// Two accumulator slots per stage (TMEM columns 128-383; G in 0-127), three
-// operand buffers: while the tensor core runs one line, the converter, the
-// two epilogues and the loads work on up to four others.  Every wait is
-// bounded by the global timer; a wait that gives up sets a CTA-wide abort
-// flag, each warp group leaves its loop together (barrier with an OR), the
-// MMA thread waits (bounded) for its MMAs, and the CTA frees its TMEM.
+//                         between the stages folded in) -> stage-2 operands in
+//                         the same pair buffer
+//   epilogue-2 warps 12-15 stage-2 accumulators -> unscaled X in a shared-
+//                         memory tile per line (128-byte swizzle), written out
+//                         by TMA tensor stores: four boxes of 16 columns x 64
+//                         rows
+// Three TMEM accumulator slots of 128 columns (G in columns 0-127); the
+// stage-1 and stage-2 accumulators of a pair share one slot, since the stage-2
+// operands exist only after the stage-1 accumulators have been read.  Every
+// wait is bounded by the global timer; a wait that gives up sets a CTA-wide
+// abort flag, each warp group leaves its loop together (barrier with an OR),
+// the MMA thread waits (bounded) for its MMAs, and the CTA frees its TMEM.
 #include "capi_internal.h"
 #include "fft_common.cuh"
 #include "tcgen05.cuh"
@@ -119,47 +123,6 @@ __device__ __forceinline__ float line_scale(float mx) {
     return ldexpf(1.f, TC_LINE_EXP - e);
 }
 
-// 8 FP32 values -> one 16-byte chunk of the operand (hi plane at b, lo plane
-// at b + 16 KB for the split; bf16 otherwise)
-template <bool SPLIT>
-__device__ __forceinline__ void store_chunk_b(uint8_t* b, uint32_t off, const float (&x)[8]) {
-    if constexpr (SPLIT) {
-        uint32_t hi[4], lo[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const __half2 h = __floats2half2_rn(x[2 * i], x[2 * i + 1]);
-            const float2 hf = __half22float2(h);
-            const __half2 l = __floats2half2_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y);
-            hi[i] = *reinterpret_cast<const uint32_t*>(&h);
-            lo[i] = *reinterpret_cast<const uint32_t*>(&l);
-        }
-        *reinterpret_cast<uint4*>(b + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-        *reinterpret_cast<uint4*>(b + 16384 + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-    } else {
-        uint32_t w[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const __nv_bfloat162 h = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
-            w[i] = *reinterpret_cast<const uint32_t*>(&h);
-        }
-        *reinterpret_cast<uint4*>(b + off) = make_uint4(w[0], w[1], w[2], w[3]);
-    }
-}
-
-// 2 FP32 values -> 4 bytes of the operand (hi/lo planes or bf16)
-template <bool SPLIT>
-__device__ __forceinline__ void store_pair_b(uint8_t* b, uint32_t off, float x0, float x1) {
-    if constexpr (SPLIT) {
-        const __half2 h = __floats2half2_rn(x0, x1);
-        const float2 hf = __half22float2(h);
-        const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
-        *reinterpret_cast<__half2*>(b + off) = h;
-        *reinterpret_cast<__half2*>(b + 16384 + off) = l;
-    } else {
-        *reinterpret_cast<__nv_bfloat162*>(b + off) = __floats2bfloat162_rn(x0, x1);
-    }
-}
-
 __device__ __forceinline__ void tma_store_2d_tc(const CUtensorMap* map, int x, int y, const void* src) {
     asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
                      reinterpret_cast<uint64_t>(map)),
@@ -173,19 +136,30 @@ __device__ __forceinline__ void prefetch_l2(const void* g, uint32_t bytes) {
 }
 
 // ---- the warp-specialised kernel --------------------------------------------
-
-constexpr int TW_CONV = 0, TW_EPI1 = 4, TW_EPI2 = 8, TW_MMA = 12;  // first warp of each role
-constexpr int TW_THREADS = 13 * 32;
-constexpr int TW_NOP = 3;    // operand buffers (stage-1 operand, then the stage-2 operand of the same line)
-constexpr int TW_ND = 2;     // accumulator slots per stage
-constexpr int TW_NS1 = 8;    // line-scale ring (the converter runs at most 5 lines ahead of epilogue 2)
-constexpr uint32_t TW_OPB = 32768;                       // one operand buffer: hi 16 KB + lo 16 KB
+//
+// Lines go through in pairs: one MMA of N = 128 covers both lines of a pair,
+// so a line costs 24 MMA instructions (split) instead of 48, and the tensor
+// core's per-instruction cost is paid once per two lines.
+constexpr int TW_CONV = 0, TW_EPI1 = 8, TW_EPI2 = 12, TW_MMA = 16;  // first warp of each role
+constexpr int TW_THREADS = 17 * 32;
+constexpr int TW_NOP = 2;    // pair operand buffers (stage-1 operands, then the stage-2 operands of the same pair)
+constexpr int TW_NSLOT = 3;  // TMEM accumulator slots of 128 columns; D1 and D2 of a pair share one
+constexpr int TW_NS1 = 8;    // line-scale ring, in pairs (the converters run at most 4 pairs ahead of epilogue 2)
+constexpr uint32_t TW_OPB = 65536;                       // one pair buffer: hi 32 KB + lo 32 KB
+constexpr uint32_t TW_LO = 32768;                        // lo plane offset inside a pair buffer
 constexpr uint32_t TW_TAB = TW_NOP * TW_OPB;             // twiddle table: 4096 float2 = 32 KB
 constexpr uint32_t TW_OUT = TW_TAB + 32768;              // two output tiles of 32 KB (4 boxes of 8 KB)
 constexpr uint32_t TW_SMEM = TW_OUT + 2 * 32768 + 1024;  // + alignment slack
 constexpr long long TW_MAX_LINES = 1LL << 24;            // per launch: output row 64*line fits in 31 bits
-constexpr uint32_t TW_GCOL = 0, TW_D1COL = 128, TW_D2COL = 256;  // TMEM columns
-constexpr int TW_BAR_CONV = 1, TW_BAR_EPI1 = 2, TW_BAR_EPI2 = 3;  // named barriers (0 is __syncthreads)
+constexpr uint32_t TW_GCOL = 0, TW_DCOL = 128;           // TMEM columns: G, then the slots
+// named barriers (0 is __syncthreads): converter group g uses 1 + g
+constexpr int TW_BAR_CONV = 1, TW_BAR_EPI1 = 3, TW_BAR_EPI2 = 4;
+// pair operand layouts (bytes inside a plane): B1 MN-major, line g's 128 K
+// rows of 128 bytes at g * 16 KB (the MMA's second 64-column N group at LBO =
+// 16 KB); B2 K-major, 128 rows (line g's k1 at row 64 g + k1), K atoms of 64
+// at 16 KB
+constexpr uint32_t B1_LINE = 16384;
+constexpr uint32_t B2P_KATOM = 16384;
 
 // bounded wait that also leaves when another role has aborted the CTA
 __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
@@ -213,16 +187,60 @@ __device__ __forceinline__ void pair_half(const float (&v)[32], int bsel, float 
     }
 }
 
+__device__ __forceinline__ void named_sync(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// 2 FP32 values -> 4 bytes of the operand (hi/lo planes at b and b + lo, or bf16)
+template <bool SPLIT>
+__device__ __forceinline__ void store_pair_p(uint8_t* b, uint32_t lo, uint32_t off, float x0, float x1) {
+    if constexpr (SPLIT) {
+        const __half2 h = __floats2half2_rn(x0, x1);
+        const float2 hf = __half22float2(h);
+        const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+        *reinterpret_cast<__half2*>(b + off) = h;
+        *reinterpret_cast<__half2*>(b + lo + off) = l;
+    } else {
+        *reinterpret_cast<__nv_bfloat162*>(b + off) = __floats2bfloat162_rn(x0, x1);
+    }
+}
+
+// 8 FP32 values -> one 16-byte chunk of the operand (hi/lo planes at b and b + lo, or bf16)
+template <bool SPLIT>
+__device__ __forceinline__ void store_chunk_p(uint8_t* b, uint32_t lo, uint32_t off, const float (&x)[8]) {
+    if constexpr (SPLIT) {
+        uint32_t hi[4], lw[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const __half2 h = __floats2half2_rn(x[2 * i], x[2 * i + 1]);
+            const float2 hf = __half22float2(h);
+            const __half2 l = __floats2half2_rn(x[2 * i] - hf.x, x[2 * i + 1] - hf.y);
+            hi[i] = *reinterpret_cast<const uint32_t*>(&h);
+            lw[i] = *reinterpret_cast<const uint32_t*>(&l);
+        }
+        *reinterpret_cast<uint4*>(b + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4*>(b + lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    } else {
+        uint32_t w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const __nv_bfloat162 h = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+            w[i] = *reinterpret_cast<const uint32_t*>(&h);
+        }
+        *reinterpret_cast<uint4*>(b + off) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
 template <bool SPLIT, bool INV>
 __global__ void __launch_bounds__(TW_THREADS, 1)
     k_fft4096_tcw(const float2* __restrict__ in, long long batch, const __grid_constant__ CUtensorMap omap,
                   const uint4* __restrict__ gplain, const float2* __restrict__ tw, int* dev_err) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t op_full1[TW_NOP], op_full2[TW_NOP], op_empty[TW_NOP];
-    __shared__ __align__(8) uint64_t d1_full[TW_ND], d1_empty[TW_ND], d2_full[TW_ND], d2_empty[TW_ND];
+    __shared__ __align__(8) uint64_t d1_full[TW_NSLOT], d2_full[TW_NSLOT], d_empty[TW_NSLOT];
     __shared__ __align__(8) uint64_t s1_full[TW_NS1], drain;
-    __shared__ float s1ring[TW_NS1];
-    __shared__ float red[2][4];
+    __shared__ float s1ring[TW_NS1][2];
+    __shared__ float red[2][2][4];  // [converter group][pair parity][warp]
     __shared__ uint32_t tmem_base_sh;
     __shared__ int abort_flag;
     volatile int* abort_sh = &abort_flag;
@@ -233,10 +251,11 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
     const uint32_t sbase = smem_u32(smem);
     float2* tab = reinterpret_cast<float2*>(smem + TW_TAB);
     constexpr uint32_t FMT = SPLIT ? 0u : 1u;
-    constexpr uint32_t IDESC1 = tc::idesc_f16(FMT, 1u, 128, 64);
-    constexpr uint32_t IDESC2 = tc::idesc_f16(FMT, 0u, 128, 64);
+    constexpr uint32_t IDESC1 = tc::idesc_f16(FMT, 1u, 128, 128);
+    constexpr uint32_t IDESC2 = tc::idesc_f16(FMT, 0u, 128, 128);
     const long long G = gridDim.x;
-    const long long nlines = batch > (long long)blockIdx.x ? (batch - blockIdx.x + G - 1) / G : 0;
+    const long long npairs = (batch + 1) / 2;
+    const long long nloc = npairs > (long long)blockIdx.x ? (npairs - blockIdx.x + G - 1) / G : 0;
 
     // T[n2*64 + k1] = W4096^(n2 k1) (times 2^-10 for the split: the stage-2
     // operand is D1 / (16 s1) * W * s1 / 64)
@@ -247,17 +266,16 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
     }
     if (tid == 0) {
         for (int j = 0; j < TW_NOP; ++j) {
-            mbar_init(&op_full1[j], 128);
+            mbar_init(&op_full1[j], 256);
             mbar_init(&op_full2[j], 128);
             mbar_init(&op_empty[j], 1);
         }
-        for (int j = 0; j < TW_ND; ++j) {
+        for (int j = 0; j < TW_NSLOT; ++j) {
             mbar_init(&d1_full[j], 1);
-            mbar_init(&d1_empty[j], 128);
             mbar_init(&d2_full[j], 1);
-            mbar_init(&d2_empty[j], 128);
+            mbar_init(&d_empty[j], 128);
         }
-        for (int j = 0; j < TW_NS1; ++j) mbar_init(&s1_full[j], 1);
+        for (int j = 0; j < TW_NS1; ++j) mbar_init(&s1_full[j], 2);
         mbar_init(&drain, 1);
         abort_flag = 0;
         fence_proxy_async_smem();
@@ -298,19 +316,27 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
     __syncthreads();
     tc::fence_after_sync();
 
-    if (warp < TW_CONV + 4) {
-        // ---------------- converter: the stage-1 operand of each line ----------------
-        const int ctid = tid;
+    if (warp < TW_CONV + 8) {
+        // ---------------- converters: group g writes line g of each pair ----------------
+        const int g = warp >> 2, wl = warp & 3, ctid = tid & 127;
 #pragma unroll 1
-        for (long long i = 0; i < nlines; ++i) {
-            const long long f = blockIdx.x + i * G;
+        for (long long i = 0; i < nloc; ++i) {
+            const long long P = blockIdx.x + i * G;
+            const long long f = 2 * P + g;
+            const bool valid = f < batch;
             const int o = (int)(i % TW_NOP);
-            if (ctid == 0 && i + 2 < nlines) prefetch_l2(in + (size_t)(f + 2 * G) * TC_N, TC_N * sizeof(float2));
-            // float4 q = ctid + 128 r holds x[2q], x[2q+1]: n1 = warp + 4 r, n2 = 2 lane (+1)
+            if (ctid == 0 && i + 2 < nloc && 2 * (P + 2 * G) + g < batch)
+                prefetch_l2(in + (size_t)(2 * (P + 2 * G) + g) * TC_N, TC_N * sizeof(float2));
+            // float4 q = ctid + 128 r holds x[2q], x[2q+1]: n1 = wl + 4 r, n2 = 2 lane (+1)
             float4 cur[16];
-            const float4* src = reinterpret_cast<const float4*>(in + (size_t)f * TC_N) + ctid;
+            if (valid) {
+                const float4* src = reinterpret_cast<const float4*>(in + (size_t)f * TC_N) + ctid;
 #pragma unroll
-            for (int r = 0; r < 16; ++r) cur[r] = __ldcs(src + 128 * r);
+                for (int r = 0; r < 16; ++r) cur[r] = __ldcs(src + 128 * r);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 16; ++r) cur[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
             if constexpr (INV) {
 #pragma unroll
                 for (int r = 0; r < 16; ++r) {
@@ -325,177 +351,190 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
                     mx = fmaxf(mx, fmaxf(fmaxf(fabsf(cur[r].x), fabsf(cur[r].y)), fmaxf(fabsf(cur[r].z), fabsf(cur[r].w))));
 #pragma unroll
                 for (int sh = 16; sh > 0; sh >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, sh));
-                if (lane == 0) red[i & 1][warp] = mx;
+                if (lane == 0) red[g][i & 1][wl] = mx;
             }
-            // the operand buffer is free once the previous user's stage-2 products are done
+            // the pair buffer is free once the previous pair's stage-2 products are done
             bool ok = true;
             if (ctid == 0) ok = wait_or_abort(&op_empty[o], (uint32_t)(((i / TW_NOP) & 1) ^ 1), abort_sh);
-            if (bar_or(TW_BAR_CONV, 128, !ok)) break;
+            if (bar_or(TW_BAR_CONV + g, 128, !ok)) break;
             float s1 = 1.f;
-            if constexpr (SPLIT) s1 = line_scale(fmaxf(fmaxf(red[i & 1][0], red[i & 1][1]), fmaxf(red[i & 1][2], red[i & 1][3])));
-            uint8_t* bp = smem + (uint32_t)o * TW_OPB;
+            if constexpr (SPLIT)
+                s1 = line_scale(fmaxf(fmaxf(red[g][i & 1][0], red[g][i & 1][1]), fmaxf(red[g][i & 1][2], red[g][i & 1][3])));
+            uint8_t* bp = smem + (uint32_t)o * TW_OPB + (uint32_t)g * B1_LINE;
             // a warp writes 64 halves (one 128-byte row) per row: no bank conflicts
 #pragma unroll
             for (int r = 0; r < 16; ++r) {
-                const int n1 = warp + 4 * r;
+                const int n1 = wl + 4 * r;
                 const float4 v = cur[r];
-                store_pair_b<SPLIT>(bp, mnmaj_off(2 * lane, 2 * n1), v.x * s1, v.z * s1);
-                store_pair_b<SPLIT>(bp, mnmaj_off(2 * lane, 2 * n1 + 1), v.y * s1, v.w * s1);
+                store_pair_p<SPLIT>(bp, TW_LO, mnmaj_off(2 * lane, 2 * n1), v.x * s1, v.z * s1);
+                store_pair_p<SPLIT>(bp, TW_LO, mnmaj_off(2 * lane, 2 * n1 + 1), v.y * s1, v.w * s1);
             }
             if (ctid == 0) {
-                s1ring[i % TW_NS1] = s1;
+                s1ring[i % TW_NS1][g] = s1;
                 mbar_arrive(&s1_full[i % TW_NS1]);
             }
             fence_proxy_async_smem();  // the operand's generic writes before the tensor core reads them
             mbar_arrive(&op_full1[o]);
         }
     } else if (warp < TW_EPI1 + 4) {
-        // ---------------- epilogue 1: twiddle and the stage-2 operand ----------------
+        // ---------------- epilogue 1: twiddle and the stage-2 operands ----------------
         const int q = warp & 3, m = 32 * q + lane;
         const int k1 = m >> 1, bsel = m & 1;
         const uint32_t lane_off = (uint32_t)(32 * q) << 16;
 #pragma unroll 1
-        for (long long i = 0; i < nlines; ++i) {
-            const int d = (int)(i % TW_ND), o = (int)(i % TW_NOP);
+        for (long long i = 0; i < nloc; ++i) {
+            const int sl = (int)(i % TW_NSLOT), o = (int)(i % TW_NOP);
             bool ok = true;
-            if (m == 0) ok = wait_or_abort(&d1_full[d], (uint32_t)((i / TW_ND) & 1), abort_sh);
+            if (m == 0) ok = wait_or_abort(&d1_full[sl], (uint32_t)((i / TW_NSLOT) & 1), abort_sh);
             if (bar_or(TW_BAR_EPI1, 128, !ok)) break;
             tc::fence_after_sync();
-            float v0[32], v1[32];
-            const uint32_t dcol = tbase + lane_off + TW_D1COL + 64 * d;
-            tc::tmem_ld32(dcol, v0);
-            tc::tmem_ld32(dcol + 32, v1);
-            tc::fence_before_sync();
-            mbar_arrive(&d1_empty[d]);  // the accumulator slot may take the next line
             uint8_t* bp = smem + (uint32_t)o * TW_OPB;
+#pragma unroll 1
+            for (int g = 0; g < 2; ++g) {
+                float v0[32], v1[32];
+                const uint32_t dcol = tbase + lane_off + TW_DCOL + 128 * sl + 64 * g;
+                tc::tmem_ld32(dcol, v0);
+                tc::tmem_ld32(dcol + 32, v1);
+                const int row = 64 * g + k1;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                float2 z[16];
-                pair_half(h ? v1 : v0, bsel, 1.f, z);
-                const int n2_0 = 32 * h + 16 * bsel;
+                for (int h = 0; h < 2; ++h) {
+                    float2 z[16];
+                    pair_half(h ? v1 : v0, bsel, 1.f, z);
+                    const int n2_0 = 32 * h + 16 * bsel;
 #pragma unroll
-                for (int j = 0; j < 16; ++j) z[j] = cmul(z[j], tab[(n2_0 + j) * 64 + k1]);
+                    for (int j = 0; j < 16; ++j) z[j] = cmul(z[j], tab[(n2_0 + j) * 64 + k1]);
 #pragma unroll
-                for (int qq = 0; qq < 4; ++qq) {
-                    float x[8];
+                    for (int qq = 0; qq < 4; ++qq) {
+                        float x[8];
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        x[2 * j] = z[4 * qq + j].x;
-                        x[2 * j + 1] = z[4 * qq + j].y;
+                        for (int j = 0; j < 4; ++j) {
+                            x[2 * j] = z[4 * qq + j].x;
+                            x[2 * j + 1] = z[4 * qq + j].y;
+                        }
+                        store_chunk_p<SPLIT>(bp, TW_LO, kmaj_off(row, 2 * (n2_0 + 4 * qq), B2P_KATOM), x);
                     }
-                    store_chunk_b<SPLIT>(bp, kmaj_off(k1, 2 * (n2_0 + 4 * qq), B2_KATOM), x);
                 }
             }
+            // D1 has been read (its slot takes this pair's D2) and the operands written
+            tc::fence_before_sync();
             fence_proxy_async_smem();
             mbar_arrive(&op_full2[o]);
         }
     } else if (warp < TW_EPI2 + 4) {
         // ---------------- epilogue 2: X out ----------------
-        // tile of line i: buffer i & 1, box bx (columns k1 = 16 bx .. 16 bx + 15)
-        // of 64 rows k2 x 128 bytes, 16-byte chunk c of row k2 at c ^ (k2 % 8)
+        // tile of line g of a pair: buffer g, box bx (columns k1 = 16 bx .. 16 bx
+        // + 15) of 64 rows k2 x 128 bytes, 16-byte chunk c of row k2 at c ^ (k2 % 8)
         // (the tensor map's 128-byte swizzle)
         const int q = warp & 3, m = 32 * q + lane;
         const int k2 = m >> 1, bsel = m & 1;
         const uint32_t lane_off = (uint32_t)(32 * q) << 16;
 #pragma unroll 1
-        for (long long i = 0; i < nlines; ++i) {
-            const long long f = blockIdx.x + i * G;
-            const int d = (int)(i % TW_ND);
-            uint8_t* ot = smem + TW_OUT + (uint32_t)(i & 1) * 32768;
+        for (long long i = 0; i < nloc; ++i) {
+            const long long P = blockIdx.x + i * G;
+            const int sl = (int)(i % TW_NSLOT);
             bool ok = true;
-            if (m == 0) {
-                ok = wait_or_abort(&d2_full[d], (uint32_t)((i / TW_ND) & 1), abort_sh) &&
+            if (m == 0)
+                ok = wait_or_abort(&d2_full[sl], (uint32_t)((i / TW_NSLOT) & 1), abort_sh) &&
                      wait_or_abort(&s1_full[i % TW_NS1], (uint32_t)((i / TW_NS1) & 1), abort_sh);
-                // the tile written two lines ago has been read by its tensor stores
-                asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-            }
             if (bar_or(TW_BAR_EPI2, 128, !ok)) break;
             tc::fence_after_sync();
-            // X = D2 / (16 s2), s2 = s1 / 64 (split); X = D2 (bf16)
-            const float s1 = s1ring[i % TW_NS1];
-            const float sc = (INV ? 1.f / (float)TC_N : 1.f) * (SPLIT ? 4.f / s1 : 1.f);
-            float v0[32], v1[32];
-            const uint32_t dcol = tbase + lane_off + TW_D2COL + 64 * d;
-            tc::tmem_ld32(dcol, v0);
-            tc::tmem_ld32(dcol + 32, v1);
-            tc::fence_before_sync();
-            mbar_arrive(&d2_empty[d]);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                float2 z[16];
-                pair_half(h ? v1 : v0, bsel, sc, z);
-                uint8_t* row = ot + (uint32_t)(2 * h + bsel) * 8192 + (uint32_t)k2 * 128;
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    float4 o4 = make_float4(z[2 * j].x, z[2 * j].y, z[2 * j + 1].x, z[2 * j + 1].y);
-                    if constexpr (INV) {
-                        o4.y = -o4.y;
-                        o4.w = -o4.w;
-                    }
-                    *reinterpret_cast<float4*>(row + ((j ^ (k2 & 7)) << 4)) = o4;
+#pragma unroll 1
+            for (int g = 0; g < 2; ++g) {
+                const long long f = 2 * P + g;
+                // X = D2 / (16 s2), s2 = s1 / 64 (split); X = D2 (bf16)
+                const float s1 = s1ring[i % TW_NS1][g];
+                const float sc = (INV ? 1.f / (float)TC_N : 1.f) * (SPLIT ? 4.f / s1 : 1.f);
+                float v0[32], v1[32];
+                const uint32_t dcol = tbase + lane_off + TW_DCOL + 128 * sl + 64 * g;
+                tc::tmem_ld32(dcol, v0);
+                tc::tmem_ld32(dcol + 32, v1);
+                if (g == 1) {
+                    tc::fence_before_sync();
+                    mbar_arrive(&d_empty[sl]);  // the slot may take a later pair
                 }
-            }
-            fence_proxy_async_smem();  // the tile's generic writes before the tensor stores read it
-            asm volatile("bar.sync %0, %1;" ::"r"(TW_BAR_EPI2), "r"(128) : "memory");
-            if (m == 0) {
+                if (f >= batch) break;  // the second line of an odd batch's last pair
+                uint8_t* ot = smem + TW_OUT + (uint32_t)g * 32768;
+                // the tile's previous tensor stores (two lines ago) have read it
+                if (m == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                named_sync(TW_BAR_EPI2, 128);
 #pragma unroll
-                for (int bx = 0; bx < 4; ++bx) tma_store_2d_tc(&omap, 32 * bx, (int)(64 * f), ot + bx * 8192);
-                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                for (int h = 0; h < 2; ++h) {
+                    float2 z[16];
+                    pair_half(h ? v1 : v0, bsel, sc, z);
+                    uint8_t* rowp = ot + (uint32_t)(2 * h + bsel) * 8192 + (uint32_t)k2 * 128;
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        float4 o4 = make_float4(z[2 * j].x, z[2 * j].y, z[2 * j + 1].x, z[2 * j + 1].y);
+                        if constexpr (INV) {
+                            o4.y = -o4.y;
+                            o4.w = -o4.w;
+                        }
+                        *reinterpret_cast<float4*>(rowp + ((j ^ (k2 & 7)) << 4)) = o4;
+                    }
+                }
+                fence_proxy_async_smem();  // the tile's generic writes before the tensor stores read it
+                named_sync(TW_BAR_EPI2, 128);
+                if (m == 0) {
+#pragma unroll
+                    for (int bx = 0; bx < 4; ++bx) tma_store_2d_tc(&omap, 32 * bx, (int)(64 * f), ot + bx * 8192);
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                }
             }
         }
         if (m == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     } else if (warp == TW_MMA && lane == 0) {
-        // ---------------- MMA issue: stage 1 of line i, stage 2 of line i - 1 ----------------
+        // ---------------- MMA issue: stage 1 of pair i, then stage 2 of pair i - 1 ----------------
         constexpr int NPROD = SPLIT ? 3 : 1;
         const uint32_t g_hi = tbase + TW_GCOL, g_lo = g_hi + 64;
         bool aborted = false;
 #pragma unroll 1
-        for (long long i = 0; i <= nlines && !aborted; ++i) {
-            if (i < nlines) {
-                const int o = (int)(i % TW_NOP), d = (int)(i % TW_ND);
+        for (long long i = 0; i <= nloc && !aborted; ++i) {
+            if (i < nloc) {
+                const int o = (int)(i % TW_NOP), sl = (int)(i % TW_NSLOT);
                 if (!wait_or_abort(&op_full1[o], (uint32_t)((i / TW_NOP) & 1), abort_sh) ||
-                    !wait_or_abort(&d1_empty[d], (uint32_t)(((i / TW_ND) & 1) ^ 1), abort_sh)) {
+                    !wait_or_abort(&d_empty[sl], (uint32_t)(((i / TW_NSLOT) & 1) ^ 1), abort_sh)) {
                     aborted = true;
                     break;
                 }
                 tc::fence_after_sync();
                 const uint32_t bb = sbase + (uint32_t)o * TW_OPB;
-                const uint32_t dd = tbase + TW_D1COL + 64 * d;
+                const uint32_t dd = tbase + TW_DCOL + 128 * sl;
 #pragma unroll
                 for (int pr = 0; pr < NPROD; ++pr) {
                     const uint32_t ga = pr == 2 ? g_lo : g_hi;
-                    const uint32_t bpl = bb + (pr == 1 ? 16384u : 0u);
+                    const uint32_t bpl = bb + (pr == 1 ? TW_LO : 0u);
 #pragma unroll
                     for (int j = 0; j < 8; ++j)
                         tc::mma_f16_ts(dd, ga + 8 * j,
-                                       tc::smem_desc(bpl + 2 * j * ATOM_SBO, 16384, ATOM_SBO, tc::LAYOUT_SW128),
+                                       tc::smem_desc(bpl + 2 * j * ATOM_SBO, B1_LINE, ATOM_SBO, tc::LAYOUT_SW128),
                                        IDESC1, (pr > 0 || j > 0) ? 1u : 0u);
                 }
-                tc::mma_commit(&d1_full[d]);
+                tc::mma_commit(&d1_full[sl]);
             }
             if (i >= 1) {
                 const long long k = i - 1;
-                const int o = (int)(k % TW_NOP), d = (int)(k % TW_ND);
-                if (!wait_or_abort(&op_full2[o], (uint32_t)((k / TW_NOP) & 1), abort_sh) ||
-                    !wait_or_abort(&d2_empty[d], (uint32_t)(((k / TW_ND) & 1) ^ 1), abort_sh)) {
+                const int o = (int)(k % TW_NOP), sl = (int)(k % TW_NSLOT);
+                // the stage-2 operands are written only after epilogue 1 has read D1,
+                // so D2 may overwrite it in the same slot
+                if (!wait_or_abort(&op_full2[o], (uint32_t)((k / TW_NOP) & 1), abort_sh)) {
                     aborted = true;
                     break;
                 }
                 tc::fence_after_sync();
                 const uint32_t bb = sbase + (uint32_t)o * TW_OPB;
-                const uint32_t dd = tbase + TW_D2COL + 64 * d;
+                const uint32_t dd = tbase + TW_DCOL + 128 * sl;
 #pragma unroll
                 for (int pr = 0; pr < NPROD; ++pr) {
                     const uint32_t ga = pr == 2 ? g_lo : g_hi;
-                    const uint32_t bpl = bb + (pr == 1 ? 16384u : 0u);
+                    const uint32_t bpl = bb + (pr == 1 ? TW_LO : 0u);
 #pragma unroll
                     for (int j = 0; j < 8; ++j)
                         tc::mma_f16_ts(dd, ga + 8 * j,
-                                       tc::smem_desc(bpl + (j / 4) * B2_KATOM + (j % 4) * 32, 16, ATOM_SBO,
+                                       tc::smem_desc(bpl + (j / 4) * B2P_KATOM + (j % 4) * 32, 16, ATOM_SBO,
                                                      tc::LAYOUT_SW128),
                                        IDESC2, (pr > 0 || j > 0) ? 1u : 0u);
                 }
-                tc::mma_commit(&d2_full[d]);
+                tc::mma_commit(&d2_full[sl]);
                 tc::mma_commit(&op_empty[o]);
             }
         }
@@ -515,8 +554,9 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
     }
 }
 
-// Launches over at most TW_MAX_LINES lines each; the output goes through a
-// tensor map of the chunk's lines as 64-row x 512-byte blocks.
+// Launches over at most TW_MAX_LINES lines each (an even count, so pairs never
+// straddle launches); the output goes through a tensor map of the chunk's
+// lines as 64-row x 512-byte blocks.
 template <bool SPLIT, bool INV>
 cudaError_t launch_tcw(const float2* in, float2* out, long long batch, const uint4* gplain, const float2* tw,
                        int* dev_err, int sms, cudaStream_t s) {
@@ -527,7 +567,8 @@ cudaError_t launch_tcw(const float2* in, float2* out, long long batch, const uin
         const long long nb = batch - b0 < TW_MAX_LINES ? batch - b0 : TW_MAX_LINES;
         CUtensorMap omap;
         if (!encode_rows(&omap, out + b0 * TC_N, (uint64_t)nb * TC_R, TC_R, 16, TC_R)) return cudaErrorInvalidValue;
-        const long long blocks = nb < sms ? nb : sms;
+        const long long pairs = (nb + 1) / 2;
+        const long long blocks = pairs < sms ? pairs : sms;
         k_fft4096_tcw<SPLIT, INV><<<(unsigned)blocks, TW_THREADS, TW_SMEM, s>>>(in + b0 * TC_N, nb, omap, gplain, tw,
                                                                                  dev_err);
         e = cudaGetLastError();
