@@ -924,7 +924,7 @@ def main():
     e2e["pageable"] = {"value": B * world * args.e2e_steps / dtp, "unit": "transforms/s",
                        "steps": args.e2e_steps, "host_memory": "pageable (numpy), same call"}
 
-    kernel_name = "k_fft_batched" if best == "fp32" else "k_fft4096_tcq"
+    kernel_name = "k_fft_batched" if best == "fp32" else "k_fft4096_tcw"
     config = tc4096_config(B)
     line = {
         "metric": METRIC,

@@ -174,6 +174,25 @@ MFFT_API int mfft_list_kernels(int64_t n, int* radix, int* lines_per_cta, int* s
 MFFT_API int mfft_plan_kernel_info(const mfft_plan* plan, int* radix, int* lines_per_cta, int* threads,
                                    int* stages);
 
+/* Four-step split (n > 16384 runs as n1-point column FFTs, a twiddle, and
+ * n2 = n/n1-point row FFTs).  The reference fixes one split per size
+ * (MetalContext.swift:57-66: 8192 = 64 x 128, 16384 = 128 x 128); here a size
+ * takes any n1 with 64 <= n1 <= 1024 and 128 <= n2 <= 1024, and plans start
+ * on the split autotuned in the context, else one read from $MFFT_TUNE_CACHE,
+ * else n1 = 2^floor(log2(n)/2).
+ *
+ * mfft_autotune_fourstep times every admissible split over `batch`
+ * transforms (<= 0: 512 MiB worth), leaves the plan on the fastest, installs
+ * it for later plans of the size in the context, appends "n n1 0 0" to
+ * $MFFT_TUNE_CACHE and reports n1.  mfft_plan_set_split pins a plan to n1
+ * (MFFT_ERR_INVALID_ARGUMENT if n1 is not admissible); mfft_plan_split reports
+ * the plan's split (0, 0 for n <= 16384); mfft_list_splits fills up to cap
+ * admissible n1 for size n and returns how many exist (host only). */
+MFFT_API int mfft_autotune_fourstep(mfft_plan* plan, int64_t batch, int* n1);
+MFFT_API int mfft_plan_set_split(mfft_plan* plan, int64_t n1);
+MFFT_API int mfft_plan_split(const mfft_plan* plan, int64_t* n1, int64_t* n2);
+MFFT_API int mfft_list_splits(int64_t n, int64_t* n1, int cap);
+
 /* ---- execution --------------------------------------------------------- */
 
 /* Batched C2C.  Replaces forward(_:) (batch = 1, MetalFFT.swift:69-85),

@@ -150,6 +150,31 @@ class MetalFFT:
         m = lib.mfft_list_kernels(n, r, f, s, 64)
         return [(r[i], f[i], s[i]) for i in range(min(m, 64))]
 
+    # ---- four-step split (n > 16384) ---------------------------------------
+    @property
+    def split(self):
+        """(n1, n2) of a four-step plan, (0, 0) for n <= 16384."""
+        n1, n2 = ctypes.c_int64(), ctypes.c_int64()
+        _check(lib.mfft_plan_split(self._plan, ctypes.byref(n1), ctypes.byref(n2)))
+        return n1.value, n2.value
+
+    def set_split(self, n1):
+        """Pin the plan to n = n1 x n/n1 (64 <= n1 <= 1024, 128 <= n/n1 <= 1024)."""
+        _check(lib.mfft_plan_set_split(self._plan, int(n1)))
+
+    def autotune_split(self, batch=0):
+        """Time every admissible split over `batch` transforms, keep the fastest, return n1."""
+        n1 = ctypes.c_int()
+        _check(lib.mfft_autotune_fourstep(self._plan, int(batch), ctypes.byref(n1)))
+        return n1.value
+
+    @staticmethod
+    def splits(n):
+        """Admissible four-step n1 values for size n ([] for n <= 16384)."""
+        buf = (ctypes.c_int64 * 8)()
+        m = lib.mfft_list_splits(int(n), buf, 8)
+        return [buf[i] for i in range(min(m, 8))]
+
     # ---- raw entry ---------------------------------------------------------
     def exec(self, inp, out, batch, direction=FORWARD, tc_variant=0):
         """Run on device tensors (torch, complex64, contiguous): out = FFT(inp)."""

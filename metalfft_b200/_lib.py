@@ -35,6 +35,10 @@ SIGNATURES = [
     ("mfft_plan_kernel_info", c_int, [c_void_p, P(c_int), P(c_int), P(c_int), P(c_int)]),
     ("mfft_plan_set_kernel", c_int, [c_void_p, c_int, c_int, c_int]),
     ("mfft_list_kernels", c_int, [c_int64, P(c_int), P(c_int), P(c_int), c_int]),
+    ("mfft_autotune_fourstep", c_int, [c_void_p, c_int64, P(c_int)]),
+    ("mfft_plan_set_split", c_int, [c_void_p, c_int64]),
+    ("mfft_plan_split", c_int, [c_void_p, P(c_int64), P(c_int64)]),
+    ("mfft_list_splits", c_int, [c_int64, P(c_int64), c_int]),
     ("mfft_exec_c2c", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),
     ("mfft_exec_c2c_backward", c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p]),
     ("mfft_exec_c2c_tc", c_int,

@@ -7,12 +7,20 @@
 // registered instantiation for the size is timed with CUDA events on a batch
 // larger than L2 and the fastest is kept.  The cache file (one line
 // "n e fpb stages" per size) is read from $MFFT_TUNE_CACHE when that is set.
+//
+// Sizes above 16384 run the four-step FFT n = n1 x n2; the reference fixes
+// n1 = 2^floor(log2(n)/2) (FourStepFFT.swift).  mfft_autotune_fourstep times
+// every admissible split (64 <= n1 <= 1024, 128 <= n2 <= 1024) and keeps the
+// fastest.
 #include <stdio.h>
 #include <stdlib.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "capi_internal.h"
+#include "fft_common.cuh"
+#include "fsqueue.h"
 
 namespace mfft {
 
@@ -111,7 +119,133 @@ int autotune_batched(mfft_ctx* ctx, int n, long long lines, const BatchedKernel*
     return MFFT_SUCCESS;
 }
 
+// Four-step splits share the cache file: a line "n n1 0 0" with n > 16384
+// records the split n = n1 x n/n1 chosen for that size.
+int fourstep_split_for(mfft_ctx* ctx, int logn) {
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        auto it = ctx->tuned_split.find(logn);
+        if (it != ctx->tuned_split.end()) return it->second;
+    }
+    int l1 = fsq_default_l1(logn);
+    int n1 = 0, z0 = 0, z1 = 0;
+    if (read_cache(1 << logn, &n1, &z0, &z1) && n1 > 0 && (n1 & (n1 - 1)) == 0 && fsq_split_ok(logn, ilog2c(n1)))
+        l1 = ilog2c(n1);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->tuned_split[logn] = l1;
+    return l1;
+}
+
+// Times the plan's four-step FFT for every admissible split over `batch`
+// transforms and leaves the plan on the fastest; the choice is installed in
+// the context for later plans of the size and appended to the cache file.
+static int autotune_split(mfft_plan* p, long long batch, int* out_l1) {
+    mfft_ctx* ctx = p->ctx;
+    const int logn = ilog2c(p->n);
+    const size_t bytes = (size_t)batch * (size_t)p->n * sizeof(float2);
+    float2 *a = nullptr, *b = nullptr;
+    if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess) {
+        cudaFree(a);
+        return set_error(MFFT_ERR_ALLOCATION, -1, -1, -1, "autotune buffers");
+    }
+    cudaMemsetAsync(a, 0, bytes, ctx->stream);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int l1_was = p->fs.l1;
+    int best = -1, st = MFFT_SUCCESS;
+    float best_ms = 1e30f;
+    for (int l1 = 6; l1 <= 10 && !st; ++l1) {
+        if (!fsq_split_ok(logn, l1)) continue;
+        st = fourstep_set_split(p, l1);
+        for (int w = 0; w < 2 && !st; ++w) st = fourstep_exec(p, a, b, batch, MFFT_FORWARD, ctx->stream, 0);
+        if (st) break;
+        cudaEventRecord(e0, ctx->stream);
+        const int reps = 6;
+        for (int r = 0; r < reps && !st; ++r)
+            st = fourstep_exec(p, (r & 1) ? b : a, (r & 1) ? a : b, batch, MFFT_FORWARD, ctx->stream, 0);
+        cudaEventRecord(e1, ctx->stream);
+        if (st) break;
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+            st = cuda_error(e, "four-step autotune");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = l1;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(a);
+    cudaFree(b);
+    if (st || best < 0) {
+        fourstep_set_split(p, l1_was);
+        return st ? st : set_error(MFFT_ERR_KERNEL_NOT_FOUND, -1, -1, -1, "no four-step split for n=%lld",
+                                   (long long)p->n);
+    }
+    st = fourstep_set_split(p, best);
+    if (st) return st;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ctx->tuned_split[logn] = best;
+    }
+    write_cache((int)p->n, 1 << best, 0, 0);
+    *out_l1 = best;
+    return MFFT_SUCCESS;
+}
+
 }  // namespace mfft
+
+extern "C" int mfft_autotune_fourstep(mfft_plan* plan, int64_t batch, int* n1) {
+    using namespace mfft;
+    if (!plan) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "plan is NULL");
+    if (plan->n <= MFFT_MAX_SINGLE_N)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "n=%lld does not use the four-step path",
+                         (long long)plan->n);
+    if (batch <= 0) batch = std::max<int64_t>(1, (int64_t)(512ll << 20) / (plan->n * 8));  // 512 MiB, 4x L2
+    DeviceGuard g(plan->ctx->device);
+    int l1 = 0;
+    int st = autotune_split(plan, batch, &l1);
+    if (st) return st;
+    if (n1) *n1 = 1 << l1;
+    return check_device_error(plan->ctx);
+}
+
+extern "C" int mfft_plan_set_split(mfft_plan* plan, int64_t n1) {
+    using namespace mfft;
+    if (!plan) return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "plan is NULL");
+    if (plan->n <= MFFT_MAX_SINGLE_N)
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "n=%lld does not use the four-step path",
+                         (long long)plan->n);
+    if (n1 <= 0 || (n1 & (n1 - 1)))
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, n1, -1, "n1 = %lld is not a power of two", (long long)n1);
+    DeviceGuard g(plan->ctx->device);
+    return fourstep_set_split(plan, ilog2c(n1));
+}
+
+extern "C" int mfft_plan_split(const mfft_plan* plan, int64_t* n1, int64_t* n2) {
+    if (!plan) return mfft::set_error(MFFT_ERR_INVALID_ARGUMENT, -1, -1, -1, "plan is NULL");
+    const bool fs = plan->n > MFFT_MAX_SINGLE_N;
+    if (n1) *n1 = fs ? plan->fs.n1 : 0;
+    if (n2) *n2 = fs ? plan->fs.n2 : 0;
+    return MFFT_SUCCESS;
+}
+
+extern "C" int mfft_list_splits(int64_t n, int64_t* n1, int cap) {
+    int m = 0;
+    if (n <= MFFT_MAX_SINGLE_N || n > MFFT_MAX_N || (n & (n - 1))) return 0;
+    const int logn = mfft::ilog2c(n);
+    for (int l1 = 6; l1 <= 10; ++l1) {
+        if (!mfft::fsq_split_ok(logn, l1)) continue;
+        if (m < cap && n1) n1[m] = 1LL << l1;
+        ++m;
+    }
+    return m;
+}
 
 extern "C" int mfft_autotune(mfft_ctx* ctx, int64_t n, int64_t lines, int* radix, int* lines_per_cta,
                              int* stages) {

@@ -30,6 +30,7 @@ struct mfft_ctx {
     std::mutex mu;
     std::map<std::pair<int, int>, float2*> twiddles;     // (n, e) -> twiddle rows
     std::map<int, const mfft::BatchedKernel*> tuned;     // n -> autotuned kernel
+    std::map<int, int> tuned_split;                      // log2 n -> autotuned log2 n1 (four-step)
     // host-array calls: a memory pool that keeps its memory between calls,
     // and the chunked pipeline of line-independent transforms (upload and
     // download streams, staging slots, one event ring per stage)
@@ -55,6 +56,7 @@ struct BatchedBinding {
 // item kernel of fsqueue.cu.
 struct FourStep {
     int n1 = 0, n2 = 0;
+    int l1 = 0;                  // log2 n1
     float2* col_tw = nullptr;    // line twiddle rows for n1 and n2
     float2* row_tw = nullptr;
     float2* tables = nullptr;    // W_N^m = fine[m % 1024] * coarse[m / 1024]
@@ -133,7 +135,6 @@ int fourstep_tables(mfft_ctx* ctx, int64_t n, float2** out);
 // Four-step sizes whose tiles move by TMA (2^16 .. 2^20), and one pass
 // (FSQ_COLS or FSQ_ROWS) of them over nb contiguous transforms of 2^logn
 // points: in / out / scratch are the first transform's data (fsqueue.h).
-bool fsq_tma_size(int logn);
 // Tensor map of `rows` rows of `row_points` complex values at `base`, boxes of
 // tile_cols complex columns x box_rows rows with the item tiles' swizzle (32,
 // 64 or 128 bytes for 4, 8 or 16 columns).
@@ -141,9 +142,14 @@ bool encode_rows(CUtensorMap* map, const float2* base, uint64_t rows, uint64_t r
                  int box_rows = 256);
 struct FsqTables;
 int fourstep_tma_pass(int kind, const FsqTables& tabs, const float2* in, float2* out, float2* scratch, long long nb,
-                      int logn, bool inv, mfft_ctx* ctx, cudaStream_t s, int adjoint = 0);
+                      int logn, int l1, bool inv, mfft_ctx* ctx, cudaStream_t s, int adjoint = 0);
 
 int fourstep_plan_init(mfft_plan* plan);
+// (Re)binds a four-step plan to the split n1 = 2^l1 (twiddle rows of n1 and n2).
+int fourstep_set_split(mfft_plan* plan, int l1);
+// The split a new four-step plan of 2^logn points takes in this context: the
+// autotuned one, else one read from $MFFT_TUNE_CACHE, else the default.
+int fourstep_split_for(mfft_ctx* ctx, int logn);
 void fourstep_plan_release(mfft_plan* plan);
 int fourstep_exec(mfft_plan* plan, const float2* in, float2* out, int64_t batch, int direction,
                   cudaStream_t s, int adjoint = 0);

@@ -70,13 +70,32 @@ int fourstep_tables(mfft_ctx* ctx, int64_t n, float2** out) {
     return MFFT_SUCCESS;
 }
 
+int fourstep_set_split(mfft_plan* p, int l1) {
+    FourStep& fs = p->fs;
+    const int logn = ilog2c(p->n);
+    if (!fsq_split_ok(logn, l1))
+        return set_error(MFFT_ERR_INVALID_ARGUMENT, -1, 1LL << l1, -1,
+                         "n1 = %d is not a valid four-step split of n = %lld (64 <= n1 <= 1024, 128 <= n/n1 <= 1024)",
+                         1 << l1, (long long)p->n);
+    int n1, n2;
+    fsq_split(logn, &n1, &n2, l1);
+    float2 *ct = nullptr, *rt = nullptr;
+    int st = line_twiddles(p->ctx, n1, &ct);
+    if (!st) st = line_twiddles(p->ctx, n2, &rt);
+    if (st) return st;
+    fs.l1 = l1;
+    fs.n1 = n1;
+    fs.n2 = n2;
+    fs.col_tw = ct;
+    fs.row_tw = rt;
+    return MFFT_SUCCESS;
+}
+
 int fourstep_plan_init(mfft_plan* p) {
     mfft_ctx* ctx = p->ctx;
     FourStep& fs = p->fs;
     const int logn = ilog2c(p->n);
-    fsq_split(logn, &fs.n1, &fs.n2);
-    int st = line_twiddles(ctx, fs.n1, &fs.col_tw);
-    if (!st) st = line_twiddles(ctx, fs.n2, &fs.row_tw);
+    int st = fourstep_set_split(p, fourstep_split_for(ctx, logn));
     if (!st) st = fourstep_tables(ctx, p->n, &fs.tables);
     if (st) return st;
     cudaError_t e = fsq_prepare();
@@ -128,17 +147,17 @@ bool encode_rows(CUtensorMap* map, const float2* base, uint64_t rows, uint64_t r
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-bool fsq_tma_size(int logn) { return logn >= 16 && logn <= 20; }
 
 int fourstep_tma_pass(int kind, const FsqTables& tabs, const float2* in, float2* out, float2* scratch, long long nb,
-                      int logn, bool inv, mfft_ctx* ctx, cudaStream_t s, int adjoint) {
+                      int logn, int l1, bool inv, mfft_ctx* ctx, cudaStream_t s, int adjoint) {
     int n1, n2;
-    fsq_split(logn, &n1, &n2);
+    fsq_split(logn, &n1, &n2, l1);
     FsqArgs a{};
     a.in = in;
     a.out = out;
     a.scratch = scratch;
     a.u_logn = logn;
+    a.u_l1 = l1;
     a.adjoint = adjoint;
     a.tabs = tabs;
     FsqMaps m{};
@@ -159,7 +178,8 @@ int fourstep_tma_pass(int kind, const FsqTables& tabs, const float2* in, float2*
 }
 
 // Column pass then row pass over chunks of up to scratch_lines transforms;
-// n = 2^16 .. 2^20 move their tiles with TMA (tile widths 4, 8 or 16).
+// splits with n1, n2 in {256, 512, 1024} move their tiles with TMA (tile
+// widths 16, 8 or 4), the others with 16-byte copies.
 int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, int direction, cudaStream_t s,
                   int adjoint) {
     const FourStep& fs = p->fs;
@@ -168,6 +188,7 @@ int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, in
     FsqArgs a{};
     a.scratch = fs.scratch;
     a.u_logn = logn;
+    a.u_l1 = fs.l1;
     a.adjoint = adjoint;
     a.tabs.line_tw[ilog2c(fs.n1) - 6] = fs.col_tw;
     a.tabs.line_tw[ilog2c(fs.n2) - 6] = fs.row_tw;
@@ -178,9 +199,12 @@ int fourstep_exec(mfft_plan* p, const float2* in, float2* out, int64_t batch, in
         const long long nb = batch - b0 < fs.scratch_lines ? batch - b0 : fs.scratch_lines;
         a.in = in + b0 * p->n;
         a.out = out + b0 * p->n;
-        if (fsq_tma_size(logn)) {
-            int st = fourstep_tma_pass(FSQ_COLS, a.tabs, a.in, a.out, a.scratch, nb, logn, inv, p->ctx, s, adjoint);
-            if (!st) st = fourstep_tma_pass(FSQ_ROWS, a.tabs, a.in, a.out, a.scratch, nb, logn, inv, p->ctx, s, adjoint);
+        if (fsq_tma_split(logn, fs.l1)) {
+            int st = fourstep_tma_pass(FSQ_COLS, a.tabs, a.in, a.out, a.scratch, nb, logn, fs.l1, inv, p->ctx, s,
+                                       adjoint);
+            if (!st)
+                st = fourstep_tma_pass(FSQ_ROWS, a.tabs, a.in, a.out, a.scratch, nb, logn, fs.l1, inv, p->ctx, s,
+                                       adjoint);
             if (st) return st;
             continue;
         }

@@ -204,7 +204,7 @@ __device__ __forceinline__ void do_rows(float2* st, const float2* mid_rows, floa
 // ---- items ----------------------------------------------------------------------
 
 struct Work {
-    int kind, logn, index, lines;
+    int kind, logn, index, lines, l1;
     long long off;      // LINES: first line; COLS / ROWS: the transform in in / out
     long long scratch;  // COLS / ROWS: the transform's intermediate
 };
@@ -219,6 +219,7 @@ __device__ __forceinline__ Work get_work(const FsqArgs& a, int p) {
         w.lines = it.lines;
         w.off = it.off;
         w.scratch = 0;
+        w.l1 = it.l1;
         if (it.kind != FSQ_LINES) {
             const FsqXform x = a.xf[it.xform];
             w.off = x.off;
@@ -231,6 +232,7 @@ __device__ __forceinline__ Work get_work(const FsqArgs& a, int p) {
     w.logn = a.u_logn;
     w.index = p - (int)(j * (unsigned)a.u_per);
     w.lines = 0;
+    w.l1 = a.u_l1;
     w.off = (long long)j << a.u_logn;
     w.scratch = w.off;
     return w;
@@ -241,7 +243,7 @@ __device__ __forceinline__ void issue(const FsqArgs& a, const Work& w, float2* s
         load_linear(st, a.in + w.off, w.lines << w.logn, true, pol);
         return;
     }
-    const int l1 = w.logn / 2, l2 = w.logn - l1;
+    const int l1 = w.l1, l2 = w.logn - l1;
     if (w.kind == FSQ_COLS) {
         const int lc = ilog2c(FSQ_POINTS) - l1;
         load_tile(st, a.in + w.off + ((long long)w.index << lc), l1, lc, 1LL << l2, pol);
@@ -267,7 +269,7 @@ __device__ __forceinline__ void compute(const FsqArgs& a, const Work& w, float2*
         }
         return;
     }
-    const int l1 = w.logn / 2, l2 = w.logn - l1;
+    const int l1 = w.l1, l2 = w.logn - l1;
     float2* mid = a.scratch + w.scratch;
     if (w.kind == FSQ_COLS) {
         const float2* tw = a.tabs.line_tw[l1 - 6];
@@ -356,7 +358,7 @@ constexpr int TMA_BOX_ROWS = 256;
 // thread 0: item p's data into stage `st`, counted on `bar`
 __device__ __forceinline__ void tma_issue(const FsqArgs& a, const FsqMaps& m, const Work& w, float2* st,
                                           uint64_t* bar) {
-    const int l1 = w.logn / 2, l2 = w.logn - l1;
+    const int l1 = w.l1, l2 = w.logn - l1;
     mbar_arrive_expect_tx(bar, FSQ_POINTS * (uint32_t)sizeof(float2));
     const long long j = w.off >> w.logn;  // transform index in this chunk
     if (w.kind == FSQ_COLS) {
@@ -374,7 +376,7 @@ __device__ __forceinline__ void tma_issue(const FsqArgs& a, const FsqMaps& m, co
 
 // thread 0: the finished tile of item w from stage `st`
 __device__ __forceinline__ void tma_store(const FsqMaps& m, const Work& w, const float2* st) {
-    const int l1 = w.logn / 2, l2 = w.logn - l1;
+    const int l1 = w.l1, l2 = w.logn - l1;
     const long long j = w.off >> w.logn;
     if (w.kind == FSQ_COLS) {
         const int lc = ilog2c(FSQ_POINTS) - l1, C = 1 << lc;
@@ -467,6 +469,7 @@ __device__ __forceinline__ Work q_work(const QDesc& d) {
     w.logn = d.logn;
     w.index = d.index;
     w.lines = d.lines;
+    w.l1 = d.l1;
     w.off = d.kind == FSQ_LINES ? d.off : d.xoff;
     w.scratch = d.kind == FSQ_LINES ? 0 : d.xscratch;
     return w;
@@ -502,7 +505,7 @@ __device__ __forceinline__ void q_issue(const FsqQueueArgs& q, const QDesc& d, f
         return;
     }
     const FsqGroupMaps& m = q.maps[it.grp];
-    const int l1 = it.logn / 2, l2 = it.logn - l1;
+    const int l1 = it.l1, l2 = it.logn - l1;
     mbar_arrive_expect_tx(bar, FSQ_POINTS * (uint32_t)sizeof(float2));
     const long long j = q_group_index(q, d);
     if (it.kind == FSQ_COLS) {
@@ -524,7 +527,7 @@ __device__ __forceinline__ void q_issue(const FsqQueueArgs& q, const QDesc& d, f
 __device__ __forceinline__ void q_tma_store(const FsqQueueArgs& q, const QDesc& d, const float2* st) {
     const FsqItem& it = d;
     const FsqGroupMaps& m = q.maps[it.grp];
-    const int l1 = it.logn / 2, l2 = it.logn - l1;
+    const int l1 = it.l1, l2 = it.logn - l1;
     const long long j = q_group_index(q, d);
     if (it.kind == FSQ_COLS) {
         const int lc = ilog2c(FSQ_POINTS) - l1, C = 1 << lc;

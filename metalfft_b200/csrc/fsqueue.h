@@ -39,13 +39,15 @@ struct alignas(16) FsqItem {
     int grp;        // queue kernel: TMA group of a COLS / ROWS item (-1: 16-byte copies)
     long long xoff;      // queue kernel, COLS / ROWS: the transform's offset in in / out
     long long xscratch;  //   and of its intermediate (the FsqXform, so one read gives both)
+    int l1;              // COLS / ROWS: log2 n1 of the transform's split
+    int pad2[3];
 };
 
 struct FsqXform {
     long long off;      // element offset of the transform in in / out
     long long scratch;  // element offset of its intermediate in the scratch buffer
     int logn;
-    int pad;
+    int l1;             // log2 n1 of its split
 };
 
 struct FsqTables {
@@ -64,33 +66,31 @@ struct FsqArgs {
     // uniform pass over `batch` contiguous four-step transforms of 2^u_logn
     // points: u_kind FSQ_COLS (pass 0) or FSQ_ROWS (pass 1), u_per items each;
     // transform j's intermediate is scratch + j * 2^u_logn
-    int u_kind, u_logn, u_per;
+    int u_kind, u_logn, u_per, u_l1;
     // 1: the adjoint of the transform (the inverse unscaled, the forward
     // scaled by 1/n); 0: the transform
     int adjoint;
     FsqTables tabs;
 };
 
-// n = 2^m (m >= 13) as n1 * n2 with n1 = 2^floor(m/2) <= n2.
-inline void fsq_split(int logn, int* n1, int* n2) {
-    *n1 = 1 << (logn / 2);
-    *n2 = 1 << (logn - logn / 2);
+// n = 2^m (m >= 13) as n1 * n2: the default n1 = 2^floor(m/2) <= n2, or a
+// split n1 = 2^l1 chosen by the autotuner.  The item kernel takes
+// 64 <= n1 <= 1024 (column FFTs) and 128 <= n2 <= 1024 (row FFTs); its TMA
+// form needs both in {256, 512, 1024} (tiles 16, 8 or 4 columns wide).
+inline int fsq_default_l1(int logn) { return logn / 2; }
+inline bool fsq_split_ok(int logn, int l1) { return l1 >= 6 && l1 <= 10 && logn - l1 >= 7 && logn - l1 <= 10; }
+inline bool fsq_tma_split(int logn, int l1) { return l1 >= 8 && l1 <= 10 && logn - l1 >= 8 && logn - l1 <= 10; }
+inline void fsq_split(int logn, int* n1, int* n2, int l1 = -1) {
+    if (l1 < 0) l1 = fsq_default_l1(logn);
+    *n1 = 1 << l1;
+    *n2 = 1 << (logn - l1);
 }
-// COLS and ROWS items of one four-step transform of 2^logn points.
-inline int fsq_cols_items(int logn) {
-    int n1, n2;
-    fsq_split(logn, &n1, &n2);
-    return n2 / (FSQ_POINTS / n1);
-}
-__host__ __device__ inline int fsq_cols_items_dev(int logn) {
-    const int n1 = 1 << (logn / 2), n2 = 1 << (logn - logn / 2);
-    return n2 / (FSQ_POINTS / n1);
-}
-inline int fsq_rows_items(int logn) {
-    int n1, n2;
-    fsq_split(logn, &n1, &n2);
-    return n1 / (FSQ_POINTS / n2);
-}
+// COLS and ROWS items of one four-step transform of 2^logn points: an item
+// holds FSQ_POINTS points (FSQ_POINTS / n1 columns of n1, or FSQ_POINTS / n2
+// rows of n2), so both passes have n / FSQ_POINTS items whatever the split.
+__host__ __device__ inline int fsq_cols_items_dev(int logn) { return (1 << logn) / FSQ_POINTS; }
+inline int fsq_cols_items(int logn) { return fsq_cols_items_dev(logn); }
+inline int fsq_rows_items(int logn) { return fsq_cols_items_dev(logn); }
 
 // Tensor maps of a uniform pass with TMA tiles: ld = the input viewed as
 // rows of n2 points (column pass), st = the column pass's intermediate (rows
@@ -116,7 +116,7 @@ struct FsqGroup {
     long long off;      // element offset of the group's first transform in in / out
     long long scratch;  // element offset of its first intermediate
     int logn;
-    int pad;
+    int l1;
 };
 struct FsqGroupMaps {
     CUtensorMap ld;    // input as rows of n2 (COLS load)

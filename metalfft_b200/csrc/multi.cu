@@ -37,7 +37,7 @@ struct mfft_multi {
     std::vector<float2*> tables;  // owned four-step W_n tables
     struct Group {                // a four-step class whose tiles move by TMA
         int64_t offset, count;
-        int logn;
+        int logn, l1;
         long long scratch;
     };
     std::vector<Group> groups;
@@ -116,10 +116,11 @@ extern "C" int mfft_multi_create(mfft_ctx* ctx, const mfft_multi_desc* descs, in
             m->tabs.fine[logn - 13] = t;
             m->tabs.coarse[logn - 13] = t + 1024;
         }
+        const int l1 = fourstep_split_for(ctx, logn);
         int grp = -1;
-        if (fsq_tma_size(logn) && (int)m->groups.size() < FSQ_MAX_GROUPS) {
+        if (fsq_tma_split(logn, l1) && (int)m->groups.size() < FSQ_MAX_GROUPS) {
             grp = (int)m->groups.size();
-            m->groups.push_back(mfft_multi::Group{d.offset, d.count, logn, scratch_pts});
+            m->groups.push_back(mfft_multi::Group{d.offset, d.count, logn, l1, scratch_pts});
         }
         const int nc = fsq_cols_items(logn), nr = fsq_rows_items(logn);
         for (int64_t j = 0; j < d.count; ++j) {
@@ -128,10 +129,13 @@ extern "C" int mfft_multi_create(mfft_ctx* ctx, const mfft_multi_desc* descs, in
             x.off = d.offset + j * d.n;
             x.scratch = scratch_pts;
             x.logn = logn;
+            x.l1 = l1;
             scratch_pts += d.n;
             xfs.push_back(x);
-            for (int c = 0; c < nc; ++c) cols.push_back(FsqItem{FSQ_COLS, logn, c, id, 0, 0, grp, x.off, x.scratch});
-            for (int r = 0; r < nr; ++r) rows.push_back(FsqItem{FSQ_ROWS, logn, r, id, 0, 0, grp, x.off, x.scratch});
+            for (int c = 0; c < nc; ++c)
+                cols.push_back(FsqItem{FSQ_COLS, logn, c, id, 0, 0, grp, x.off, x.scratch, l1, {0, 0, 0}});
+            for (int r = 0; r < nr; ++r)
+                rows.push_back(FsqItem{FSQ_ROWS, logn, r, id, 0, 0, grp, x.off, x.scratch, l1, {0, 0, 0}});
         }
     }
     if (st) {
@@ -183,9 +187,9 @@ static int multi_device(mfft_multi* m, const float2* in, float2* out, int direct
     for (int gi = 0; gi < q.ngroups; ++gi) {
         const auto& g = m->groups[gi];
         int n1, n2;
-        fsq_split(g.logn, &n1, &n2);
+        fsq_split(g.logn, &n1, &n2, g.l1);
         const int C = FSQ_POINTS / n1, RW = FSQ_POINTS / n2;
-        q.groups[gi] = FsqGroup{g.offset, g.scratch, g.logn, 0};
+        q.groups[gi] = FsqGroup{g.offset, g.scratch, g.logn, g.l1};
         FsqGroupMaps& mp = q.maps[gi];
         if (!encode_rows(&mp.ld, in + g.offset, (uint64_t)g.count * n1, n2, C) ||
             !encode_rows(&mp.stc, m->scratch + g.scratch, (uint64_t)g.count * n1, n2, C) ||

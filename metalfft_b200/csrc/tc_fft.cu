@@ -72,9 +72,8 @@ constexpr int TC_LINE_EXP = 14;     // FP16 split: line scaled so |max| < 2^14
 // Operand layouts: 128-byte swizzle (1024-byte atoms of 8 rows x 128 bytes,
 // 16-byte chunk c of row r stored at chunk c ^ (r % 8)), so that the eight
 // threads of a quarter-warp storing one 128-byte row hit distinct banks.
-//  B1 (B, MN-major): rows = K (128), N = n2 (64 = one 128-byte row)
-//  B2 (B, K-major):  rows n = k1 (64), K = 2*n2+a (128) = 2 atoms of 64
-constexpr uint32_t B2_KATOM = 8192;   //  8 row groups x 1024
+//  B1 (B, MN-major): rows = K (128), N = n2 (64 = one 128-byte row per line)
+//  B2 (B, K-major):  rows n = k1 (64 per line), K = 2*n2+a (128) = 2 atoms of 64
 constexpr uint32_t ATOM_SBO = 1024;   // stride of 8-row groups
 
 __host__ __device__ constexpr uint32_t sw128(uint32_t row, uint32_t chunk) {
@@ -177,13 +176,17 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
 
 // lane m of the calling warp's quarter: pairs (row 2k, row 2k+1) of 32
 // accumulator columns into 16 complex values z[i] (column 16*b + i of the
-// half), scaled by s
+// half), scaled by s.  With SWAP the odd lanes (b = 1) get their columns in
+// the order i ^ 8, so that the two lanes of a pair write different 16-byte
+// chunks of a shared-memory row at the same step.
+template <bool SWAP = false>
 __device__ __forceinline__ void pair_half(const float (&v)[32], int bsel, float s, float2 (&z)[16]) {
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
-        const float send = bsel ? v[i] : v[16 + i];
+        constexpr int X = SWAP ? 8 : 0;
+        const float send = bsel ? v[i] : v[16 + (i ^ X)];
         const float r = __shfl_xor_sync(0xffffffffu, send, 1);
-        z[i] = bsel ? make_float2(r * s, v[16 + i] * s) : make_float2(v[i] * s, r * s);
+        z[i] = bsel ? make_float2(r * s, v[16 + (i ^ X)] * s) : make_float2(v[i] * s, r * s);
     }
 }
 
@@ -257,10 +260,13 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
     const long long npairs = (batch + 1) / 2;
     const long long nloc = npairs > (long long)blockIdx.x ? (npairs - blockIdx.x + G - 1) / G : 0;
 
-    // T[n2*64 + k1] = W4096^(n2 k1) (times 2^-10 for the split: the stage-2
-    // operand is D1 / (16 s1) * W * s1 / 64)
+    // T[n2*64 + (k1 + 8 * bit 4 of n2) % 64] = W4096^(n2 k1) (times 2^-10 for
+    // the split: the stage-2 operand is D1 / (16 s1) * W * s1 / 64).  The
+    // rotation puts rows n2 and n2 + 16, which the two lanes of a pair read at
+    // the same step, on different banks.
     for (int i = tid; i < TC_N; i += TW_THREADS) {
-        const float2 w = __ldg(tw + (((i >> 6) * (i & 63)) & (TC_N - 1)));
+        const int n2 = i >> 6, k1 = ((i & 63) - 8 * ((n2 >> 4) & 1)) & 63;
+        const float2 w = __ldg(tw + ((n2 * k1) & (TC_N - 1)));
         const float sc = SPLIT ? 0.0009765625f : 1.f;
         tab[i] = make_float2(w.x * sc, w.y * sc);
     }
@@ -402,7 +408,7 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
                     pair_half(h ? v1 : v0, bsel, 1.f, z);
                     const int n2_0 = 32 * h + 16 * bsel;
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) z[j] = cmul(z[j], tab[(n2_0 + j) * 64 + k1]);
+                    for (int j = 0; j < 16; ++j) z[j] = cmul(z[j], tab[(n2_0 + j) * 64 + ((k1 + 8 * bsel) & 63)]);
 #pragma unroll
                     for (int qq = 0; qq < 4; ++qq) {
                         float x[8];
@@ -460,8 +466,9 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     float2 z[16];
-                    pair_half(h ? v1 : v0, bsel, sc, z);
+                    pair_half<true>(h ? v1 : v0, bsel, sc, z);
                     uint8_t* rowp = ot + (uint32_t)(2 * h + bsel) * 8192 + (uint32_t)k2 * 128;
+                    const int xr = (k2 & 7) ^ (4 * bsel);  // odd lanes hold chunk j ^ 4 at step j
 #pragma unroll
                     for (int j = 0; j < 8; ++j) {
                         float4 o4 = make_float4(z[2 * j].x, z[2 * j].y, z[2 * j + 1].x, z[2 * j + 1].y);
@@ -469,7 +476,7 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
                             o4.y = -o4.y;
                             o4.w = -o4.w;
                         }
-                        *reinterpret_cast<float4*>(rowp + ((j ^ (k2 & 7)) << 4)) = o4;
+                        *reinterpret_cast<float4*>(rowp + ((j ^ xr) << 4)) = o4;
                     }
                 }
                 fence_proxy_async_smem();  // the tile's generic writes before the tensor stores read it

@@ -45,6 +45,22 @@ def test_status_strings_and_host_helpers():
     assert lib.mfft_recommended_fft_size(16384) == 0
 
 
+def test_four_step_split_lists():
+    """Admissible splits n = n1 x n2 (64 <= n1 <= 1024, 128 <= n2 <= 1024) of
+    the four-step sizes; none below 32768."""
+    from metalfft_b200 import _lib
+    lib = _lib.load()
+    buf = (ctypes.c_int64 * 8)()
+    want = {1 << 15: [64, 128, 256], 1 << 16: [64, 128, 256, 512], 1 << 17: [128, 256, 512, 1024],
+            1 << 18: [256, 512, 1024], 1 << 19: [512, 1024], 1 << 20: [1024]}
+    for n, w in want.items():
+        m = lib.mfft_list_splits(n, buf, 8)
+        assert list(buf[:m]) == w, n
+    for n in (4096, 16384, 1 << 21, 3 << 15):
+        assert lib.mfft_list_splits(n, buf, 8) == 0
+    assert lib.mfft_list_splits(1 << 16, buf, 2) == 4  # count beyond cap
+
+
 def test_no_device_is_reported_not_faked():
     import torch
     if torch.cuda.is_available():
