@@ -77,7 +77,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv", "fconv", "sar", "sarfocus", "stft",
-                                                        "psd", "xspec"])
+                                                        "psd", "xspec", "fourstep", "c2c4096sweep"])
     return p.parse_args()
 
 
@@ -348,13 +348,22 @@ def cpu_baseline_other(workload, seconds=8.0):
     from oracle import oracle as O
     from metalfft_b200 import workloads
     rng = np.random.default_rng(SEED)
-    if workload == "c2c4096x256":
+    if workload in ("c2c4096x256", "c2c4096sweep"):
         x = O.uniform_c64((256, 4096), SEED)
 
         def fn():
             O.ref_fft(O.ref_fft(x), inverse=True)
         units, unit = 512, "transforms/s"
         what = "256 lines of N=4096, forward then inverse, FP32 radix-4 Stockham restatement"
+    elif workload == "fourstep":
+        sample = [(1 << l, max(1, (1 << 19) >> l)) for l in range(15, 21)]
+        xs = [O.normal_c64((c, n), SEED + i) for i, (n, c) in enumerate(sample)]
+
+        def fn():
+            for x in xs:
+                O.ref_fft(x)
+        units, unit = sum(n * c for n, c in sample), "points/s"
+        what = "2^19 points of each size 2^15..2^20, FP32 four-step restatement"
     elif workload == "mixed":
         # every size class, lines capped at 2^18 points per class
         sample = [(n, max(1, min(c, (1 << 18) // n))) for n, c in workloads.mixed_size_classes()]
@@ -554,6 +563,85 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
                                   "frac": gbs / peak, "peak_source": peak_src,
                                   "note": "16 B per point algorithmic; four-step lines move 32 B"},
                      "gpu_launches": 4 * args.steps, "clocks": clk})
+    elif args.workload == "c2c4096sweep":
+        # config 1's step (one CUDA graph: forward, then inverse) over a range
+        # of batches; a least-squares line through the per-launch times splits
+        # them into a fixed cost per launch and a cost per line
+        n = 4096
+        f = M.MetalFFT(n)
+        sweep, clk = {}, None
+        for b in (32, 64, 128, 256, 512, 1024, 2048, 4096):
+            sets = max(2, (1 << 30) // (b * n * 8))  # >= 1 GiB of rotating buffers, > L2
+            xs = torch.randn(sets, b, n, dtype=torch.complex64, device="cuda")
+            ys = torch.empty_like(xs)
+            graphs = [f.capture([(xs[k], ys[k], b, M.FORWARD), (ys[k], xs[k], b, M.INVERSE)])
+                      for k in range(sets)]
+            ms_max, ms, c = timed(lambda i: graphs[i % sets].replay(), args.steps, args.warmup, barrier,
+                                  dist, uuid)
+            clk = clk or c
+            us = ms_max / args.steps / 2 * 1e3
+            sweep[b] = {"us_per_launch": us, "frac": b * n * 16 / (us / 1e6) / 1e9 / peak}
+            del graphs, xs, ys
+        bs = np.array(sorted(sweep), np.float64)
+        ts = np.array([sweep[b]["us_per_launch"] for b in sorted(sweep)])
+        slope, icpt = np.polyfit(bs, ts, 1)
+        us256 = sweep[256]["us_per_launch"]
+        gbs = 256 * n * 16 / (us256 / 1e6) / 1e9
+        line.update({"metric": "batched C2C FFT N=4096 x 256: transforms/s (forward + inverse), batch sweep",
+                     "value": 2 * 256 * world / (2 * us256 / 1e6), "unit": "transforms/s",
+                     "ms_per_step": 2 * us256 / 1e3, "sweep": sweep,
+                     "fit": {"fixed_us_per_launch": icpt, "ns_per_line": slope * 1e3,
+                             "lines_per_s_marginal": 1e6 / slope,
+                             "note": "least squares over the batches: per-launch time = fixed + lines x per-line"},
+                     "config": {"workload": "C2C FFT N=4096, batches 32..4096, N(0,1), forward then inverse "
+                                            "in one CUDA graph", "l2": ">= 1 GiB of rotating buffer sets"},
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak, "peak_source": peak_src},
+                     "gpu_launches": 16 * args.steps, "clocks": clk})
+    elif args.workload == "fourstep":
+        # every admissible split n = n1 x n2 of each four-step size, 2^25
+        # points (256 MiB in, 256 MiB out) per launch, then the autotuner
+        pts = 1 << 25
+        x = torch.from_numpy(workloads.normal_c64(pts, SEED + rank)).cuda()
+        y = torch.empty_like(x)
+        table, best_ms, default_ms, auto = {}, 0.0, 0.0, {}
+        clk = None
+        for l in range(15, 21):
+            n = 1 << l
+            b = pts // n
+            f = M.MetalFFT(n)
+            n1_default = f.split[0]
+            row = {}
+            for n1 in M.MetalFFT.splits(n):
+                f.set_split(n1)
+                ms_max, ms, c = timed(lambda i: f.exec(x, y, b, M.FORWARD), args.steps, args.warmup, barrier,
+                                      dist, uuid)
+                row[n1] = ms_max / args.steps
+                clk = clk or c
+            f.set_split(min(row, key=row.get))
+            f.exec(x, y, b, M.FORWARD)
+            torch.cuda.synchronize()
+            err = fp64_check(x[:2 * n].view(2, n).cpu().numpy(), y[:2 * n].view(2, n).cpu().numpy())
+            g = M.MetalFFT(n)
+            auto[n] = g.autotune_split(batch=b)
+            table[n] = {"ms_per_launch": row, "default_n1": n1_default, "autotuned_n1": auto[n],
+                        "rel_rms": err}
+            best_ms += min(row.values())
+            default_ms += row[n1_default]
+        assert M.lib.mfft_context_check(M.shared_context()) == 0
+        gbs = 6 * pts * 16 / (best_ms / 1e3) / 1e9
+        line.update({"metric": "four-step FFT, sizes 2^15..2^20, 2^25 points each: points/s (fastest split)",
+                     "value": 6 * pts * world / (best_ms / 1e3), "unit": "points/s",
+                     "ms_per_step": best_ms,
+                     "default_split_points_per_s": 6 * pts * world / (default_ms / 1e3),
+                     "splits": table,
+                     "config": {"workload": "one forward launch of 2^25 complex64 N(0,1) points per size, "
+                                            "every admissible split n1 (64..1024, n/n1 in 128..1024)",
+                                "l2": "256 MiB in + 256 MiB out per launch > L2"},
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak, "peak_source": peak_src,
+                                  "note": "16 B per point algorithmic; the intermediate adds 16 B"},
+                     "gpu_launches": 12 * args.steps, "clocks": clk})
     elif args.workload in ("stft", "psd"):
         if args.workload == "stft":
             n, fft, hop = 1 << 24, 1024, 512
