@@ -11,8 +11,10 @@
 //   stage 2  X[k1 + 64 k2] = sum_n2 W64^(n2 k2) Z[n2][k1]      tensor cores
 //
 // Each product is D (128 x 64, FP32 in TMEM) = G (128 x 128) * B (128 x 64):
-// G is the realified DFT-64 matrix, row 2k+b = component b (re/im) of output
-// k, column 2n+a = component a of input n; B holds one line's data with the
+// G is the realified DFT-64 matrix, row 16 (k / 8) + 8 b + k % 8 = component
+// b (re/im) of output k (so the two components of an output sit 8 TMEM lanes
+// apart, where one thread of a 16-lane TMEM load receives both), column 2n+a
+// = component a of input n; B holds one line's data with the
 // same interleaved re/im index along K.  G is the A operand, K-major, held in
 // tensor memory for the whole kernel (lane m = row m, two 16-bit K values per
 // 32-bit column); the line is the B operand in shared memory: MN-major for
@@ -34,9 +36,10 @@
 //                         pair: coalesced 16-byte streaming loads (the pair
 //                         two ahead prefetched into L2), the line's power-of-
 //                         two scale, its stage-1 operand (hi/lo) into one of
-//                         two 64 KB pair buffers
-//   MMA warp 16 (1 thread) stage-1 products of pair i, then stage-2 products
-//                         of pair i-1; the DFT-64 operand G lives in tensor
+//                         three 64 KB pair buffers
+//   MMA warp 16 (1 thread) stage-1 products of a pair, or stage-2 products of
+//                         an earlier pair, whichever has its operands first;
+//                         the DFT-64 operand G lives in tensor
 //                         memory (the A operand), so the tensor core reads
 //                         only the operands from shared memory
 //   epilogue-1 warps 8-11 stage-1 accumulators (TMEM) -> re/im pairs -> times
@@ -44,9 +47,12 @@
 //                         between the stages folded in) -> stage-2 operands in
 //                         the same pair buffer
 //   epilogue-2 warps 12-15 stage-2 accumulators -> unscaled X in a shared-
-//                         memory tile per line (128-byte swizzle), written out
-//                         by TMA tensor stores: four boxes of 16 columns x 64
-//                         rows
+//                         memory tile per line (128-byte swizzle) inside the
+//                         pair's own buffer (its operands have been consumed
+//                         once the stage-2 products complete), written out by
+//                         TMA tensor stores: four boxes of 16 columns x 64
+//                         rows; the buffer goes back to the converters once
+//                         the stores have read it
 // Three TMEM accumulator slots of 128 columns (G in columns 0-127); the
 // stage-1 and stage-2 accumulators of a pair share one slot, since the stage-2
 // operands exist only after the stage-1 accumulators have been read.  Every
@@ -89,14 +95,14 @@ __host__ __device__ constexpr uint32_t mnmaj_off(uint32_t nn, uint32_t kk) {
 }
 
 // Tables (FP64 sincospi): G = realified DFT-64 as plain row-major 16-bit
-// planes (row m = 2k+b, column kk = 2n+a; FP16 hi and lo of 16 * G, and
+// planes (row m = 16 (k / 8) + 8 b + k % 8, column kk = 2n+a; FP16 hi and lo of 16 * G, and
 // BF16 of G) -- the image each lane stores into tensor memory -- and
 // T[m] = W4096^m.
 __global__ void k_tc_tables(__half* g_hi, __half* g_lo, __nv_bfloat16* g_bf, float2* tw) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;  // 0 .. 128*128-1
     if (idx < 128 * 128) {
         const int m = idx / 128, kk = idx % 128;
-        const int k = m >> 1, b = m & 1, n = kk >> 1, a = kk & 1;
+        const int k = 8 * (m >> 4) + (m & 7), b = (m >> 3) & 1, n = kk >> 1, a = kk & 1;
         double s, c;
         sincospi(-2.0 * (double)((n * k) % TC_R) / (double)TC_R, &s, &c);  // W64^(nk) = c + i s
         // out re = c*xr - s*xi ; out im = s*xr + c*xi
@@ -141,18 +147,21 @@ __device__ __forceinline__ void prefetch_l2(const void* g, uint32_t bytes) {
 // core's per-instruction cost is paid once per two lines.
 constexpr int TW_CONV = 0, TW_EPI1 = 8, TW_EPI2 = 12, TW_MMA = 16;  // first warp of each role
 constexpr int TW_THREADS = 17 * 32;
-constexpr int TW_NOP = 2;    // pair operand buffers (stage-1 operands, then the stage-2 operands of the same pair)
+// pair buffers: the stage-1 operands, then the stage-2 operands, then the two
+// lines' output tiles of the same pair
+constexpr int TW_NOP = 3;
 constexpr int TW_NSLOT = 3;  // TMEM accumulator slots of 128 columns; D1 and D2 of a pair share one
-constexpr int TW_NS1 = 8;    // line-scale ring, in pairs (the converters run at most 4 pairs ahead of epilogue 2)
+constexpr int TW_PF = 2;     // L2 prefetch distance of the converters, in pairs
+constexpr int TW_NS1 = 8;    // line-scale ring, in pairs (the converters run at most 3 pairs ahead of epilogue 2)
 constexpr uint32_t TW_OPB = 65536;                       // one pair buffer: hi 32 KB + lo 32 KB
 constexpr uint32_t TW_LO = 32768;                        // lo plane offset inside a pair buffer
 constexpr uint32_t TW_TAB = TW_NOP * TW_OPB;             // twiddle table: 4096 float2 = 32 KB
-constexpr uint32_t TW_OUT = TW_TAB + 32768;              // two output tiles of 32 KB (4 boxes of 8 KB)
-constexpr uint32_t TW_SMEM = TW_OUT + 2 * 32768 + 1024;  // + alignment slack
+constexpr uint32_t TW_SMEM = TW_TAB + 32768 + 1024;      // + alignment slack
 constexpr long long TW_MAX_LINES = 1LL << 24;            // per launch: output row 64*line fits in 31 bits
 constexpr uint32_t TW_GCOL = 0, TW_DCOL = 128;           // TMEM columns: G, then the slots
-// named barriers (0 is __syncthreads): converter group g uses 1 + g
-constexpr int TW_BAR_CONV = 1, TW_BAR_EPI1 = 3, TW_BAR_EPI2 = 4;
+// named barriers (0 is __syncthreads): converter group g uses 1 + g; 5 joins the
+// epilogue and MMA warps once the table and G are set up
+constexpr int TW_BAR_CONV = 1, TW_BAR_EPI1 = 3, TW_BAR_EPI2 = 4, TW_BAR_SETUP = 5;
 // pair operand layouts (bytes inside a plane): B1 MN-major, line g's 128 K
 // rows of 128 bytes at g * 16 KB (the MMA's second 64-column N group at LBO =
 // 16 KB); B2 K-major, 128 rows (line g's k1 at row 64 g + k1), K atoms of 64
@@ -174,22 +183,6 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
     return true;
 }
 
-// lane m of the calling warp's quarter: pairs (row 2k, row 2k+1) of 32
-// accumulator columns into 16 complex values z[i] (column 16*b + i of the
-// half), scaled by s.  With SWAP the odd lanes (b = 1) get their columns in
-// the order i ^ 8, so that the two lanes of a pair write different 16-byte
-// chunks of a shared-memory row at the same step.
-template <bool SWAP = false>
-__device__ __forceinline__ void pair_half(const float (&v)[32], int bsel, float s, float2 (&z)[16]) {
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        constexpr int X = SWAP ? 8 : 0;
-        const float send = bsel ? v[i] : v[16 + (i ^ X)];
-        const float r = __shfl_xor_sync(0xffffffffu, send, 1);
-        z[i] = bsel ? make_float2(r * s, v[16 + (i ^ X)] * s) : make_float2(v[i] * s, r * s);
-    }
-}
-
 __device__ __forceinline__ void named_sync(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
@@ -206,6 +199,22 @@ __device__ __forceinline__ void store_pair_p(uint8_t* b, uint32_t lo, uint32_t o
     } else {
         *reinterpret_cast<__nv_bfloat162*>(b + off) = __floats2bfloat162_rn(x0, x1);
     }
+}
+
+// Column orders of the two products (the N index of each MMA), chosen so that
+// every shared-memory access of the converters and the epilogues is free of
+// bank conflicts for the 16-lane TMEM load layout:
+//   stage 1: column j = 8 r + 2 c + s holds n2 = s + 2 r0 + 4 r1 + 8 c + 32 r2
+//            (r = r2 r1 r0 in bits), so a lane's steps 2 rp, 2 rp + 1 cover four
+//            consecutive n2, one 16-byte chunk of the stage-2 operand;
+//   stage 2: output k1 sits in column stage2_col(k1) (bits 1, 2, 3 of k1 moved
+//            to 3, 1, 2), so that column j = 8 r + 2 c + s holds
+//            k1 = 16 (r / 2) + 4 c + 2 (r % 2) + s.
+__host__ __device__ constexpr int stage1_col(int n2) {  // inverse of the stage-1 order, n2 -> column
+    return (n2 & 1) | (((n2 >> 3) & 3) << 1) | (((n2 >> 1) & 1) << 3) | (((n2 >> 2) & 1) << 4) | (((n2 >> 5) & 1) << 5);
+}
+__host__ __device__ constexpr int stage2_col(int k1) {
+    return (k1 & 1) | (((k1 >> 2) & 1) << 1) | (((k1 >> 3) & 1) << 2) | (((k1 >> 1) & 1) << 3) | (k1 & 48);
 }
 
 // 8 FP32 values -> one 16-byte chunk of the operand (hi/lo planes at b and b + lo, or bf16)
@@ -250,26 +259,19 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
+    const long long G = gridDim.x;
+    const long long npairs = (batch + 1) / 2;
+    const long long nloc = npairs > (long long)blockIdx.x ? (npairs - blockIdx.x + G - 1) / G : 0;
+    // the first TW_PF pairs into L2 while the CTA sets up
+    if (tid < 2 * TW_PF && tid / 2 < nloc && 2 * (blockIdx.x + (tid / 2) * G) + (tid & 1) < batch)
+        prefetch_l2(in + (size_t)(2 * (blockIdx.x + (tid / 2) * G) + (tid & 1)) * TC_N, TC_N * sizeof(float2));
     uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const uint32_t sbase = smem_u32(smem);
     float2* tab = reinterpret_cast<float2*>(smem + TW_TAB);
     constexpr uint32_t FMT = SPLIT ? 0u : 1u;
     constexpr uint32_t IDESC1 = tc::idesc_f16(FMT, 1u, 128, 128);
     constexpr uint32_t IDESC2 = tc::idesc_f16(FMT, 0u, 128, 128);
-    const long long G = gridDim.x;
-    const long long npairs = (batch + 1) / 2;
-    const long long nloc = npairs > (long long)blockIdx.x ? (npairs - blockIdx.x + G - 1) / G : 0;
 
-    // T[n2*64 + (k1 + 8 * bit 4 of n2) % 64] = W4096^(n2 k1) (times 2^-10 for
-    // the split: the stage-2 operand is D1 / (16 s1) * W * s1 / 64).  The
-    // rotation puts rows n2 and n2 + 16, which the two lanes of a pair read at
-    // the same step, on different banks.
-    for (int i = tid; i < TC_N; i += TW_THREADS) {
-        const int n2 = i >> 6, k1 = ((i & 63) - 8 * ((n2 >> 4) & 1)) & 63;
-        const float2 w = __ldg(tw + ((n2 * k1) & (TC_N - 1)));
-        const float sc = SPLIT ? 0.0009765625f : 1.f;
-        tab[i] = make_float2(w.x * sc, w.y * sc);
-    }
     if (tid == 0) {
         for (int j = 0; j < TW_NOP; ++j) {
             mbar_init(&op_full1[j], 256);
@@ -295,6 +297,22 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
     tc::fence_after_sync();
     const uint32_t tbase = tmem_base_sh;
 
+    // The epilogue and MMA warps set up the twiddle table and G while the
+    // converters start on the first pair.
+    if (warp >= TW_EPI1) {
+        // T[n2*64 + (k1 + 4 * ((n2 >> 3) & 3)) % 64] = W4096^(n2 k1) (times 2^-10
+        // for the split: the stage-2 operand is D1 / (16 s1) * W * s1 / 64).  A
+        // half-warp of epilogue 1 reads 4 consecutive k1 of the rows n2 = n + 8c,
+        // c = 0..3; the rotation puts the four rows on distinct banks.
+        if (warp < TW_EPI2 + 4) {
+            for (int i = tid - 32 * TW_EPI1; i < TC_N; i += 256) {
+                const int n2 = i >> 6, k1 = ((i & 63) - 4 * ((n2 >> 3) & 3)) & 63;
+                const float2 w = __ldg(tw + ((n2 * k1) & (TC_N - 1)));
+                const float sc = SPLIT ? 0.0009765625f : 1.f;
+                tab[i] = make_float2(w.x * sc, w.y * sc);
+            }
+        }
+    }
     // G into tensor memory: lane m holds row m (hi in columns 0-63, lo in 64-127)
     if (warp >= TW_EPI1 && warp < TW_EPI1 + 4) {
         const int m = 32 * (warp & 3) + lane;
@@ -318,9 +336,11 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
             }
         }
     }
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
+    if (warp >= TW_EPI1) {
+        tc::fence_before_sync();
+        named_sync(TW_BAR_SETUP, 32 * (TW_MMA + 1 - TW_EPI1));
+        tc::fence_after_sync();
+    }
 
     if (warp < TW_CONV + 8) {
         // ---------------- converters: group g writes line g of each pair ----------------
@@ -330,9 +350,9 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
             const long long P = blockIdx.x + i * G;
             const long long f = 2 * P + g;
             const bool valid = f < batch;
-            const int o = (int)(i % TW_NOP);
-            if (ctid == 0 && i + 2 < nloc && 2 * (P + 2 * G) + g < batch)
-                prefetch_l2(in + (size_t)(2 * (P + 2 * G) + g) * TC_N, TC_N * sizeof(float2));
+            const int o = (int)i % TW_NOP;
+            if (ctid == 0 && i + TW_PF < nloc && 2 * (P + TW_PF * G) + g < batch)
+                prefetch_l2(in + (size_t)(2 * (P + TW_PF * G) + g) * TC_N, TC_N * sizeof(float2));
             // float4 q = ctid + 128 r holds x[2q], x[2q+1]: n1 = wl + 4 r, n2 = 2 lane (+1)
             float4 cur[16];
             if (valid) {
@@ -361,66 +381,85 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
             }
             // the pair buffer is free once the previous pair's stage-2 products are done
             bool ok = true;
-            if (ctid == 0) ok = wait_or_abort(&op_empty[o], (uint32_t)(((i / TW_NOP) & 1) ^ 1), abort_sh);
+            if (ctid == 0) ok = wait_or_abort(&op_empty[o], (uint32_t)((((int)i / TW_NOP) & 1) ^ 1), abort_sh);
             if (bar_or(TW_BAR_CONV + g, 128, !ok)) break;
             float s1 = 1.f;
             if constexpr (SPLIT)
                 s1 = line_scale(fmaxf(fmaxf(red[g][i & 1][0], red[g][i & 1][1]), fmaxf(red[g][i & 1][2], red[g][i & 1][3])));
             uint8_t* bp = smem + (uint32_t)o * TW_OPB + (uint32_t)g * B1_LINE;
-            // a warp writes 64 halves (one 128-byte row) per row: no bank conflicts
+            // columns j, j + 1 of the operand take n2 = 2 lane, 2 lane + 1 (the
+            // stage-1 column order); a warp writes one 128-byte row per row: no
+            // bank conflicts
+            const int j0 = stage1_col(2 * lane);
 #pragma unroll
             for (int r = 0; r < 16; ++r) {
                 const int n1 = wl + 4 * r;
                 const float4 v = cur[r];
-                store_pair_p<SPLIT>(bp, TW_LO, mnmaj_off(2 * lane, 2 * n1), v.x * s1, v.z * s1);
-                store_pair_p<SPLIT>(bp, TW_LO, mnmaj_off(2 * lane, 2 * n1 + 1), v.y * s1, v.w * s1);
+                store_pair_p<SPLIT>(bp, TW_LO, mnmaj_off(j0, 2 * n1), v.x * s1, v.z * s1);
+                store_pair_p<SPLIT>(bp, TW_LO, mnmaj_off(j0, 2 * n1 + 1), v.y * s1, v.w * s1);
             }
             if (ctid == 0) {
-                s1ring[i % TW_NS1][g] = s1;
-                mbar_arrive(&s1_full[i % TW_NS1]);
+                s1ring[(int)i % TW_NS1][g] = s1;
+                mbar_arrive(&s1_full[(int)i % TW_NS1]);
             }
             fence_proxy_async_smem();  // the operand's generic writes before the tensor core reads them
             mbar_arrive(&op_full1[o]);
         }
     } else if (warp < TW_EPI1 + 4) {
         // ---------------- epilogue 1: twiddle and the stage-2 operands ----------------
-        const int q = warp & 3, m = 32 * q + lane;
-        const int k1 = m >> 1, bsel = m & 1;
-        const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+        // 16-lane TMEM loads: half hb of the warp's lane quarter q gives lane
+        // (rl = lane / 4) the real and imaginary rows of k1 = 16 q + 8 hb + rl,
+        // columns j = 8 r + 2 c + s (c = lane % 4, r = 0..7, s = 0, 1), which
+        // hold n2 = stage1_n2(j)
+        const int q = warp & 3, m = 32 * q + lane, rl = lane >> 2, c = lane & 3;
+        const uint32_t lane_q = (uint32_t)(32 * q) << 16;
+        const int rot = 4 * c;  // table rotation of this lane's rows n2 (bits 3-4 of n2 = c)
 #pragma unroll 1
         for (long long i = 0; i < nloc; ++i) {
-            const int sl = (int)(i % TW_NSLOT), o = (int)(i % TW_NOP);
+            const int sl = (int)i % TW_NSLOT, o = (int)i % TW_NOP;
             bool ok = true;
-            if (m == 0) ok = wait_or_abort(&d1_full[sl], (uint32_t)((i / TW_NSLOT) & 1), abort_sh);
+            if (m == 0) ok = wait_or_abort(&d1_full[sl], (uint32_t)(((int)i / TW_NSLOT) & 1), abort_sh);
             if (bar_or(TW_BAR_EPI1, 128, !ok)) break;
             tc::fence_after_sync();
             uint8_t* bp = smem + (uint32_t)o * TW_OPB;
-#pragma unroll 1
-            for (int g = 0; g < 2; ++g) {
-                float v0[32], v1[32];
-                const uint32_t dcol = tbase + lane_off + TW_DCOL + 128 * sl + 64 * g;
-                tc::tmem_ld32(dcol, v0);
-                tc::tmem_ld32(dcol + 32, v1);
-                const int row = 64 * g + k1;
+            // block gh = (line g, lane half hb) = (gh / 2, gh % 2); the load of
+            // block gh + 1 is in flight while block gh is processed
+            auto taddr = [&](int gh) {
+                return tbase + lane_q + ((uint32_t)(16 * (gh & 1)) << 16) + TW_DCOL + 128 * sl + 64 * (gh >> 1);
+            };
+            auto proc = [&](const uint32_t(&v)[32], int gh) {
+                const int k1 = 16 * q + 8 * (gh & 1) + rl;
+                const int row = 64 * (gh >> 1) + stage2_col(k1);
+                const float2* trow = tab + ((k1 + rot) & 63);
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    float2 z[16];
-                    pair_half(h ? v1 : v0, bsel, 1.f, z);
-                    const int n2_0 = 32 * h + 16 * bsel;
+                for (int rp = 0; rp < 4; ++rp) {
+                    // steps r = 2 rp, 2 rp + 1 hold n2 = nb .. nb + 3: one 16-byte chunk (K = 2 nb .. 2 nb + 7)
+                    const int nb = 4 * (rp & 1) + 8 * c + 32 * (rp >> 1);
+                    float x[8];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) z[j] = cmul(z[j], tab[(n2_0 + j) * 64 + ((k1 + 8 * bsel) & 63)]);
-#pragma unroll
-                    for (int qq = 0; qq < 4; ++qq) {
-                        float x[8];
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            x[2 * j] = z[4 * qq + j].x;
-                            x[2 * j + 1] = z[4 * qq + j].y;
-                        }
-                        store_chunk_p<SPLIT>(bp, TW_LO, kmaj_off(row, 2 * (n2_0 + 4 * qq), B2P_KATOM), x);
+                    for (int t = 0; t < 4; ++t) {
+                        const int r = 2 * rp + (t >> 1), sb = t & 1;
+                        const float2 z = cmul(make_float2(__uint_as_float(v[4 * r + sb]), __uint_as_float(v[4 * r + 2 + sb])),
+                                              trow[(nb + t) * 64]);
+                        x[2 * t] = z.x;
+                        x[2 * t + 1] = z.y;
                     }
+                    store_chunk_p<SPLIT>(bp, TW_LO, kmaj_off(row, 2 * nb, B2P_KATOM), x);
                 }
-            }
+            };
+            uint32_t va[32], vb[32];
+            tc::tmem_ld16x256_issue(taddr(0), va);
+            tc::tmem_wait_ld(va);
+            tc::tmem_ld16x256_issue(taddr(1), vb);
+            proc(va, 0);
+            tc::tmem_wait_ld(vb);
+            tc::tmem_ld16x256_issue(taddr(2), va);
+            proc(vb, 1);
+            tc::tmem_wait_ld(va);
+            tc::tmem_ld16x256_issue(taddr(3), vb);
+            proc(va, 2);
+            tc::tmem_wait_ld(vb);
+            proc(vb, 3);
             // D1 has been read (its slot takes this pair's D2) and the operands written
             tc::fence_before_sync();
             fence_proxy_async_smem();
@@ -428,121 +467,155 @@ __global__ void __launch_bounds__(TW_THREADS, 1)
         }
     } else if (warp < TW_EPI2 + 4) {
         // ---------------- epilogue 2: X out ----------------
-        // tile of line g of a pair: buffer g, box bx (columns k1 = 16 bx .. 16 bx
-        // + 15) of 64 rows k2 x 128 bytes, 16-byte chunk c of row k2 at c ^ (k2 % 8)
-        // (the tensor map's 128-byte swizzle)
-        const int q = warp & 3, m = 32 * q + lane;
-        const int k2 = m >> 1, bsel = m & 1;
-        const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+        // 16-lane TMEM loads as in epilogue 1: lane (rl, c) gets X[k1 + 64 k2] for
+        // k2 = 16 q + 8 hb + rl and the stage-2 column j = 8 r + 2 c + s, which
+        // holds k1 = 16 (r / 2) + 4 c + 2 (r % 2) + s.  Tile of line g: bytes
+        // [32 KB g, 32 KB (g + 1)) of the pair buffer, box bx (columns k1 = 16 bx
+        // .. 16 bx + 15) of 64 rows k2 x 128 bytes, 16-byte chunk ch of row k2 at
+        // ch ^ (k2 % 8) (the tensor map's 128-byte swizzle)
+        const int q = warp & 3, m = 32 * q + lane, rl = lane >> 2, c = lane & 3;
+        const uint32_t lane_q = (uint32_t)(32 * q) << 16;
 #pragma unroll 1
         for (long long i = 0; i < nloc; ++i) {
             const long long P = blockIdx.x + i * G;
-            const int sl = (int)(i % TW_NSLOT);
+            const int sl = (int)i % TW_NSLOT, o = (int)i % TW_NOP;
             bool ok = true;
             if (m == 0)
-                ok = wait_or_abort(&d2_full[sl], (uint32_t)((i / TW_NSLOT) & 1), abort_sh) &&
-                     wait_or_abort(&s1_full[i % TW_NS1], (uint32_t)((i / TW_NS1) & 1), abort_sh);
+                ok = wait_or_abort(&d2_full[sl], (uint32_t)(((int)i / TW_NSLOT) & 1), abort_sh) &&
+                     wait_or_abort(&s1_full[(int)i % TW_NS1], (uint32_t)(((int)i / TW_NS1) & 1), abort_sh);
             if (bar_or(TW_BAR_EPI2, 128, !ok)) break;
             tc::fence_after_sync();
-#pragma unroll 1
-            for (int g = 0; g < 2; ++g) {
-                const long long f = 2 * P + g;
-                // X = D2 / (16 s2), s2 = s1 / 64 (split); X = D2 (bf16)
-                const float s1 = s1ring[i % TW_NS1][g];
-                const float sc = (INV ? 1.f / (float)TC_N : 1.f) * (SPLIT ? 4.f / s1 : 1.f);
-                float v0[32], v1[32];
-                const uint32_t dcol = tbase + lane_off + TW_DCOL + 128 * sl + 64 * g;
-                tc::tmem_ld32(dcol, v0);
-                tc::tmem_ld32(dcol + 32, v1);
-                if (g == 1) {
-                    tc::fence_before_sync();
-                    mbar_arrive(&d_empty[sl]);  // the slot may take a later pair
-                }
-                if (f >= batch) break;  // the second line of an odd batch's last pair
-                uint8_t* ot = smem + TW_OUT + (uint32_t)g * 32768;
-                // the tile's previous tensor stores (two lines ago) have read it
-                if (m == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-                named_sync(TW_BAR_EPI2, 128);
+            // the stage-2 products have completed, so the pair buffer takes the
+            // two output tiles (line g at g * 32 KB); block gh = (line g, lane half
+            // hb) = (gh / 2, gh % 2), the load of block gh + 1 in flight while block
+            // gh is processed
+            uint8_t* bp = smem + (uint32_t)o * TW_OPB;
+            auto taddr = [&](int gh) {
+                return tbase + lane_q + ((uint32_t)(16 * (gh & 1)) << 16) + TW_DCOL + 128 * sl + 64 * (gh >> 1);
+            };
+            // X = D2 / (16 s2), s2 = s1 / 64 (split); X = D2 (bf16)
+            const float sc0 = (INV ? 1.f / (float)TC_N : 1.f) * (SPLIT ? 4.f / s1ring[(int)i % TW_NS1][0] : 1.f);
+            const float sc1 = (INV ? 1.f / (float)TC_N : 1.f) * (SPLIT ? 4.f / s1ring[(int)i % TW_NS1][1] : 1.f);
+            const bool live1 = 2 * P + 1 < batch;  // false for the second line of an odd batch's last pair
+            auto proc = [&](const uint32_t(&v)[32], int gh) {
+                const int g = gh >> 1;
+                const float sc = g ? sc1 : sc0;
+                const int k2 = 16 * q + 8 * (gh & 1) + rl;
+                uint8_t* rowp = bp + (uint32_t)g * 32768 + (uint32_t)k2 * 128;
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    float2 z[16];
-                    pair_half<true>(h ? v1 : v0, bsel, sc, z);
-                    uint8_t* rowp = ot + (uint32_t)(2 * h + bsel) * 8192 + (uint32_t)k2 * 128;
-                    const int xr = (k2 & 7) ^ (4 * bsel);  // odd lanes hold chunk j ^ 4 at step j
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        float4 o4 = make_float4(z[2 * j].x, z[2 * j].y, z[2 * j + 1].x, z[2 * j + 1].y);
-                        if constexpr (INV) {
-                            o4.y = -o4.y;
-                            o4.w = -o4.w;
-                        }
-                        *reinterpret_cast<float4*>(rowp + ((j ^ xr) << 4)) = o4;
+                for (int r = 0; r < 8; ++r) {
+                    float4 o4 = make_float4(__uint_as_float(v[4 * r]) * sc, __uint_as_float(v[4 * r + 2]) * sc,
+                                            __uint_as_float(v[4 * r + 1]) * sc, __uint_as_float(v[4 * r + 3]) * sc);
+                    if constexpr (INV) {
+                        o4.y = -o4.y;
+                        o4.w = -o4.w;
                     }
+                    const int ch = (r & 1) + 2 * c;  // X[k1], X[k1 + 1], k1 = 16 (r / 2) + 4 c + 2 (r % 2)
+                    *reinterpret_cast<float4*>(rowp + (uint32_t)(r >> 1) * 8192 + ((ch ^ (k2 & 7)) << 4)) = o4;
                 }
+            };
+            // line g's tile is complete: four tensor stores of its boxes
+            auto store_line = [&](int g) {
                 fence_proxy_async_smem();  // the tile's generic writes before the tensor stores read it
                 named_sync(TW_BAR_EPI2, 128);
                 if (m == 0) {
+                    const uint8_t* ot = bp + (uint32_t)g * 32768;
 #pragma unroll
-                    for (int bx = 0; bx < 4; ++bx) tma_store_2d_tc(&omap, 32 * bx, (int)(64 * f), ot + bx * 8192);
+                    for (int bx = 0; bx < 4; ++bx) tma_store_2d_tc(&omap, 32 * bx, (int)(64 * (2 * P + g)), ot + bx * 8192);
                     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                 }
+            };
+            uint32_t va[32], vb[32];
+            tc::tmem_ld16x256_issue(taddr(0), va);
+            tc::tmem_wait_ld(va);
+            tc::tmem_ld16x256_issue(taddr(1), vb);
+            proc(va, 0);
+            tc::tmem_wait_ld(vb);
+            tc::tmem_ld16x256_issue(taddr(2), va);
+            proc(vb, 1);
+            store_line(0);
+            tc::tmem_wait_ld(va);
+            tc::tmem_ld16x256_issue(taddr(3), vb);
+            if (live1) proc(va, 2);
+            tc::tmem_wait_ld(vb);
+            tc::fence_before_sync();
+            mbar_arrive(&d_empty[sl]);  // the slot may take a later pair
+            if (live1) {
+                proc(vb, 3);
+                store_line(1);
+            }
+            // the pair buffer goes back to the converters once the tensor stores have read it
+            if (m == 0) {
+                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                mbar_arrive(&op_empty[o]);
             }
         }
         if (m == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     } else if (warp == TW_MMA && lane == 0) {
-        // ---------------- MMA issue: stage 1 of pair i, then stage 2 of pair i - 1 ----------------
+        // ---------------- MMA issue ----------------
+        // Stage 1 of pair i1 and stage 2 of pair i2 < i1, whichever has its
+        // operands first (stage 2 first when both do), so that the tensor core
+        // runs the ready stage while the other's operands are still being made.
         constexpr int NPROD = SPLIT ? 3 : 1;
         const uint32_t g_hi = tbase + TW_GCOL, g_lo = g_hi + 64;
         bool aborted = false;
+        long long i1 = 0, i2 = 0;
+        uint64_t t0 = globaltimer_ns();
 #pragma unroll 1
-        for (long long i = 0; i <= nloc && !aborted; ++i) {
-            if (i < nloc) {
-                const int o = (int)(i % TW_NOP), sl = (int)(i % TW_NSLOT);
-                if (!wait_or_abort(&op_full1[o], (uint32_t)((i / TW_NOP) & 1), abort_sh) ||
-                    !wait_or_abort(&d_empty[sl], (uint32_t)(((i / TW_NSLOT) & 1) ^ 1), abort_sh)) {
-                    aborted = true;
-                    break;
-                }
-                tc::fence_after_sync();
-                const uint32_t bb = sbase + (uint32_t)o * TW_OPB;
-                const uint32_t dd = tbase + TW_DCOL + 128 * sl;
-#pragma unroll
-                for (int pr = 0; pr < NPROD; ++pr) {
-                    const uint32_t ga = pr == 2 ? g_lo : g_hi;
-                    const uint32_t bpl = bb + (pr == 1 ? TW_LO : 0u);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        tc::mma_f16_ts(dd, ga + 8 * j,
-                                       tc::smem_desc(bpl + 2 * j * ATOM_SBO, B1_LINE, ATOM_SBO, tc::LAYOUT_SW128),
-                                       IDESC1, (pr > 0 || j > 0) ? 1u : 0u);
-                }
-                tc::mma_commit(&d1_full[sl]);
-            }
-            if (i >= 1) {
-                const long long k = i - 1;
-                const int o = (int)(k % TW_NOP), sl = (int)(k % TW_NSLOT);
+        while (i2 < nloc) {
+            bool issued = false;
+            if (i2 < i1) {
+                const int o = (int)i2 % TW_NOP, sl = (int)i2 % TW_NSLOT;
                 // the stage-2 operands are written only after epilogue 1 has read D1,
                 // so D2 may overwrite it in the same slot
-                if (!wait_or_abort(&op_full2[o], (uint32_t)((k / TW_NOP) & 1), abort_sh)) {
-                    aborted = true;
-                    break;
-                }
-                tc::fence_after_sync();
-                const uint32_t bb = sbase + (uint32_t)o * TW_OPB;
-                const uint32_t dd = tbase + TW_DCOL + 128 * sl;
+                if (mbar_test_wait(&op_full2[o], (uint32_t)(((int)i2 / TW_NOP) & 1))) {
+                    tc::fence_after_sync();
+                    const uint32_t bb = sbase + (uint32_t)o * TW_OPB;
+                    const uint32_t dd = tbase + TW_DCOL + 128 * sl;
 #pragma unroll
-                for (int pr = 0; pr < NPROD; ++pr) {
-                    const uint32_t ga = pr == 2 ? g_lo : g_hi;
-                    const uint32_t bpl = bb + (pr == 1 ? TW_LO : 0u);
+                    for (int pr = 0; pr < NPROD; ++pr) {
+                        const uint32_t ga = pr == 2 ? g_lo : g_hi;
+                        const uint32_t bpl = bb + (pr == 1 ? TW_LO : 0u);
 #pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        tc::mma_f16_ts(dd, ga + 8 * j,
-                                       tc::smem_desc(bpl + (j / 4) * B2P_KATOM + (j % 4) * 32, 16, ATOM_SBO,
-                                                     tc::LAYOUT_SW128),
-                                       IDESC2, (pr > 0 || j > 0) ? 1u : 0u);
+                        for (int j = 0; j < 8; ++j)
+                            tc::mma_f16_ts(dd, ga + 8 * j,
+                                           tc::smem_desc(bpl + (j / 4) * B2P_KATOM + (j % 4) * 32, 16, ATOM_SBO,
+                                                         tc::LAYOUT_SW128),
+                                           IDESC2, (pr > 0 || j > 0) ? 1u : 0u);
+                    }
+                    tc::mma_commit(&d2_full[sl]);
+                    ++i2;
+                    issued = true;
                 }
-                tc::mma_commit(&d2_full[sl]);
-                tc::mma_commit(&op_empty[o]);
+            }
+            if (!issued && i1 < nloc) {
+                const int o = (int)i1 % TW_NOP, sl = (int)i1 % TW_NSLOT;
+                if (mbar_test_wait(&op_full1[o], (uint32_t)(((int)i1 / TW_NOP) & 1)) &&
+                    mbar_test_wait(&d_empty[sl], (uint32_t)((((int)i1 / TW_NSLOT) & 1) ^ 1))) {
+                    tc::fence_after_sync();
+                    const uint32_t bb = sbase + (uint32_t)o * TW_OPB;
+                    const uint32_t dd = tbase + TW_DCOL + 128 * sl;
+#pragma unroll
+                    for (int pr = 0; pr < NPROD; ++pr) {
+                        const uint32_t ga = pr == 2 ? g_lo : g_hi;
+                        const uint32_t bpl = bb + (pr == 1 ? TW_LO : 0u);
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            tc::mma_f16_ts(dd, ga + 8 * j,
+                                           tc::smem_desc(bpl + 2 * j * ATOM_SBO, B1_LINE, ATOM_SBO, tc::LAYOUT_SW128),
+                                           IDESC1, (pr > 0 || j > 0) ? 1u : 0u);
+                    }
+                    tc::mma_commit(&d1_full[sl]);
+                    ++i1;
+                    issued = true;
+                }
+            }
+            if (issued) {
+                t0 = globaltimer_ns();
+            } else if (*abort_sh || globaltimer_ns() - t0 > WAIT_LIMIT_NS) {
+                *abort_sh = 1;
+                aborted = true;
+                break;
             }
         }
         if (aborted) {
