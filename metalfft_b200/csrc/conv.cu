@@ -124,13 +124,19 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, ConvGeom<FFT>::MINB_FW
             if (i < lim1) im = __ldcs(xb + hop + i);
             v[m] = make_float2(re, im);
         }
-        fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
+        // forward transform, times H, inverse transform through one call site
+        // (two inlined transforms get interleaved and need more registers)
+#pragma unroll 1
+        for (int ph = 0; ph < 2; ++ph) {
+            fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
+            if (ph == 0) {
 #pragma unroll
-        for (int m = 0; m < CONV_E; ++m) {
-            const float2 h = __ldg(H + t + m * T);
-            v[m] = cconj(cmul(v[m], h));  // conj for the inverse
+                for (int m = 0; m < CONV_E; ++m) {
+                    const float2 h = __ldg(H + t + m * T);
+                    v[m] = cconj(cmul(v[m], h));  // conj for the inverse
+                }
+            }
         }
-        fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
         // v[m] = conj(FFT * FFT) -> r = conj(v)/FFT; re = block b, im = block b+1
         const bool write = active && p >= p0;
         float* yb = y + base;
@@ -209,50 +215,54 @@ __global__ void __launch_bounds__(ConvGeom<FFT>::THREADS, 1)
     for (int it = 0; it < blocks_per_unit; it += 2) {
         const int off0 = it * hop, off1 = off0 + hop;
         const bool a0 = it < mine, a1 = it + 1 < mine;
-        float2 v[CONV_E];
-        {
-            const int l0 = a0 ? clamp_count(ny_u - off0, FFT) : 0;
-            const int l1 = a1 ? clamp_count(ny_u - off1, FFT) : 0;
+        const int ly0 = a0 ? clamp_count(ny_u - off0, FFT) : 0, ly1 = a1 ? clamp_count(ny_u - off1, FFT) : 0;
+        const int lx0 = a0 ? clamp_count(nx_u - off0, hop) : 0, lx1 = a1 ? clamp_count(nx_u - off1, hop) : 0;
+        // The three transforms of a block pair go through one call site (phase
+        // 0: Z, 1: dx, 2: W), so that the compiler does not interleave their
+        // code, which needs more registers than a thread of 512 has.
+#pragma unroll 1
+        for (int ph = 0; ph < 3; ++ph) {
+            if (ph == 1 && !du) continue;  // the same for every thread
+            float2 v[CONV_E];
+            if (ph == 0) {
 #pragma unroll
-            for (int m = 0; m < CONV_E; ++m) {
-                const int i = t + m * T;
-                v[m] = make_float2(i < l0 ? __ldcs(gu + off0 + i) : 0.f, i < l1 ? __ldcs(gu + off1 + i) : 0.f);
-            }
-        }
-        fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
+                for (int m = 0; m < CONV_E; ++m) {
+                    const int i = t + m * T;
+                    v[m] = make_float2(i < ly0 ? __ldcs(gu + off0 + i) : 0.f, i < ly1 ? __ldcs(gu + off1 + i) : 0.f);
+                }
+            } else if (ph == 1) {
+                // conj(Z conj H): the inverse as a forward transform of the conjugate
 #pragma unroll
-        for (int m = 0; m < CONV_E; ++m) Zs[t + m * T] = v[m];
-        {
-            const int l0 = a0 ? clamp_count(nx_u - off0, hop) : 0;
-            const int l1 = a1 ? clamp_count(nx_u - off1, hop) : 0;
+                for (int m = 0; m < CONV_E; ++m) {
+                    const int k = t + m * T;
+                    v[m] = cconj(cmul(Zs[k], cconj(__ldg(H + k))));
+                }
+            } else {
 #pragma unroll
-            for (int m = 0; m < CONV_E; ++m) {
-                const int i = t + m * T;
-                v[m] = make_float2(i < l0 ? __ldcs(xu + off0 + i) : 0.f, i < l1 ? __ldcs(xu + off1 + i) : 0.f);
-            }
-        }
-        fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
-#pragma unroll
-        for (int m = 0; m < CONV_E; ++m) {
-            const int k = t + m * T;
-            D[k] = cadd(D[k], cmul(Zs[k], cconj(v[m])));
-        }
-        if (du) {
-            // conj(Z conj H): the inverse as a forward transform of the conjugate
-#pragma unroll
-            for (int m = 0; m < CONV_E; ++m) {
-                const int k = t + m * T;
-                v[m] = cconj(cmul(Zs[k], cconj(__ldg(H + k))));
+                for (int m = 0; m < CONV_E; ++m) {
+                    const int i = t + m * T;
+                    v[m] = make_float2(i < lx0 ? __ldcs(xu + off0 + i) : 0.f, i < lx1 ? __ldcs(xu + off1 + i) : 0.f);
+                }
             }
             fft_regs<FFT, CONV_E, G::WS>(v, t, buf, tw);
-            const int l0 = a0 ? clamp_count(nx_u - off0, hop) : 0;
-            const int l1 = a1 ? clamp_count(nx_u - off1, hop) : 0;
+            if (ph == 0) {
 #pragma unroll
-            for (int m = 0; m < CONV_E; ++m) {
-                const int i = t + m * T;
-                // IFFT = conj(FFT(conj)) / FFT: re = block b, im = block b+1
-                if (i < l0) __stcs(du + off0 + i, v[m].x * sc);
-                if (i < l1) __stcs(du + off1 + i, -v[m].y * sc);
+                for (int m = 0; m < CONV_E; ++m) Zs[t + m * T] = v[m];
+            } else if (ph == 1) {
+#pragma unroll
+                for (int m = 0; m < CONV_E; ++m) {
+                    const int i = t + m * T;
+                    // IFFT = conj(FFT(conj)) / FFT: re = block b, im = block b+1
+                    if (i < lx0) __stcs(du + off0 + i, v[m].x * sc);
+                    if (i < lx1) __stcs(du + off1 + i, -v[m].y * sc);
+                }
+            } else {
+                // P += Z conj(W) (each thread owns its bins)
+#pragma unroll
+                for (int m = 0; m < CONV_E; ++m) {
+                    const int k = t + m * T;
+                    D[k] = cadd(D[k], cmul(Zs[k], cconj(v[m])));
+                }
             }
         }
     }
