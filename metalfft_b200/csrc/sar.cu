@@ -229,10 +229,16 @@ __global__ void __launch_bounds__(NR / SAR_E) k_sar_range(const __half2* __restr
     float2 v[SAR_E];
 #pragma unroll
     for (int m = 0; m < SAR_E; ++m) v[m] = cmul(__half22float2(rawp[m * T]), rot);
-    fft_regs<NR, SAR_E, (T <= 32)>(v, t, PadLine{smem}, tw);
+    // forward transform, times conj(H), inverse transform through one call site
+    // (two inlined transforms get interleaved and need more registers)
+#pragma unroll 1
+    for (int ph = 0; ph < 2; ++ph) {
+        fft_regs<NR, SAR_E, (T <= 32)>(v, t, PadLine{smem}, tw);
+        if (ph == 0) {
 #pragma unroll
-    for (int m = 0; m < SAR_E; ++m) v[m] = cconj(cmul(v[m], __ldg(H + t + m * T)));
-    fft_regs<NR, SAR_E, (T <= 32)>(v, t, PadLine{smem}, tw);
+            for (int m = 0; m < SAR_E; ++m) v[m] = cconj(cmul(v[m], __ldg(H + t + m * T)));
+        }
+    }
     float mx = 0.f;
     const float inv_n = 1.f / (float)NR;
 #pragma unroll
@@ -286,42 +292,50 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
         const float s = __ldg(rc_scale + p);
         v[m] = make_float2(u.x * s, INV ? -u.y * s : u.y * s);
     }
-    fft_regs<NA, SAR_E, false>(v, t, ColLine<C>{smem, c}, tw);  // v[m] = I[k = t + m*T][col]
-    if constexpr (INV) {
-        // inverse transform along azimuth: conj(FFT(conj(x))) / NA
-        const float sc = 1.0f / (float)NA;
+    // the azimuth transform and, for the gradient, the transform of conj(G)
+    // through one call site (two inlined transforms get interleaved and need
+    // more registers)
+    double lsum = 0.0;
+#pragma unroll 1
+    for (int ph = 0; ph < (GRAD ? 2 : 1); ++ph) {
+        fft_regs<NA, SAR_E, false>(v, t, ColLine<C>{smem, c}, tw);  // ph 0: v[m] = I[k = t + m*T][col]
+        if (ph == 1) break;                                          // ph 1: v[m] = conj(B[p]), p = t + m*T
+        if constexpr (INV) {
+            // inverse transform along azimuth: conj(FFT(conj(x))) / NA
+            const float sc = 1.0f / (float)NA;
 #pragma unroll
-        for (int m = 0; m < SAR_E; ++m) v[m] = make_float2(v[m].x * sc, -v[m].y * sc);
-    }
-    if constexpr (IMAGE) {
-        float mx = 0.f;
+            for (int m = 0; m < SAR_E; ++m) v[m] = make_float2(v[m].x * sc, -v[m].y * sc);
+        }
+        if constexpr (IMAGE) {
+            float mx = 0.f;
 #pragma unroll
-        for (int m = 0; m < SAR_E; ++m) mx = fmaxf(mx, fmaxf(fabsf(v[m].x), fabsf(v[m].y)));
-        // max over the T threads of column c: lanes differing in t share a warp
-        // when C < 32 (t varies across lane bits above log2 C)
+            for (int m = 0; m < SAR_E; ++m) mx = fmaxf(mx, fmaxf(fabsf(v[m].x), fabsf(v[m].y)));
+            // max over the T threads of column c: lanes differing in t share a warp
+            // when C < 32 (t varies across lane bits above log2 C)
 #pragma unroll
-        for (int o = 16; o >= C; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        const int w = threadIdx.x >> 5;
-        if ((threadIdx.x & 31) < C) red[w][c] = mx;
-        __syncthreads();
-        float cm = 0.f;
-        for (int i = 0; i < (AzGeom<NA>::THREADS + 31) / 32; ++i) cm = fmaxf(cm, red[i][c]);
-        const float s = block_scale(cm);
-        const float inv = 1.f / s;
-        __half2* icol = image + (long long)t * nr + col;
+            for (int o = 16; o >= C; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            const int w = threadIdx.x >> 5;
+            if ((threadIdx.x & 31) < C) red[w][c] = mx;
+            __syncthreads();
+            float cm = 0.f;
+            for (int i = 0; i < (AzGeom<NA>::THREADS + 31) / 32; ++i) cm = fmaxf(cm, red[i][c]);
+            const float s = block_scale(cm);
+            const float inv = 1.f / s;
+            __half2* icol = image + (long long)t * nr + col;
 #pragma unroll
-        for (int m = 0; m < SAR_E; ++m) icol[m * rstep] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
-        if (t == 0) image_scale[col] = s;
+            for (int m = 0; m < SAR_E; ++m) icol[m * rstep] = __floats2half2_rn(v[m].x * inv, v[m].y * inv);
+            if (t == 0) image_scale[col] = s;
+        }
+        if constexpr (GRAD) {
+#pragma unroll
+            for (int m = 0; m < SAR_E; ++m) {
+                const float a2 = v[m].x * v[m].x + v[m].y * v[m].y;
+                lsum += (double)a2 * (double)a2;
+                v[m] = make_float2(4.f * a2 * v[m].x, -4.f * a2 * v[m].y);  // conj(G)
+            }
+        }
     }
     if constexpr (GRAD) {
-        double lsum = 0.0;
-#pragma unroll
-        for (int m = 0; m < SAR_E; ++m) {
-            const float a2 = v[m].x * v[m].x + v[m].y * v[m].y;
-            lsum += (double)a2 * (double)a2;
-            v[m] = make_float2(4.f * a2 * v[m].x, -4.f * a2 * v[m].y);  // conj(G)
-        }
-        fft_regs<NA, SAR_E, false>(v, t, ColLine<C>{smem, c}, tw);  // conj(B[p]), p = t + m*T
         float d[SAR_E];
 #pragma unroll
         for (int m = 0; m < SAR_E; ++m) {
