@@ -76,6 +76,8 @@ def parse():
     p.add_argument("--batch", type=int, default=BATCH)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--fs-log2", default="15-20",
+                   help="fourstep workload: log2 sizes to sweep, a range lo-hi or one value")
     p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv", "fconv", "sar", "sarfocus", "stft",
                                                         "psd", "xspec", "fourstep", "c2c4096sweep"])
     return p.parse_args()
@@ -605,8 +607,10 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
         x = torch.from_numpy(workloads.normal_c64(pts, SEED + rank)).cuda()
         y = torch.empty_like(x)
         table, best_ms, default_ms, auto = {}, 0.0, 0.0, {}
-        clk = None
-        for l in range(15, 21):
+        clk, launches = None, 0
+        lo, _, hi = args.fs_log2.partition("-")
+        sizes = range(int(lo), int(hi or lo) + 1)
+        for l in sizes:
             n = 1 << l
             b = pts // n
             f = M.MetalFFT(n)
@@ -618,6 +622,7 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
                                       dist, uuid)
                 row[n1] = ms_max / args.steps
                 clk = clk or c
+                launches += 2 * args.steps  # column pass + row pass per call
             f.set_split(min(row, key=row.get))
             f.exec(x, y, b, M.FORWARD)
             torch.cuda.synchronize()
@@ -629,11 +634,12 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
             best_ms += min(row.values())
             default_ms += row[n1_default]
         assert M.lib.mfft_context_check(M.shared_context()) == 0
-        gbs = 6 * pts * 16 / (best_ms / 1e3) / 1e9
-        line.update({"metric": "four-step FFT, sizes 2^15..2^20, 2^25 points each: points/s (fastest split)",
-                     "value": 6 * pts * world / (best_ms / 1e3), "unit": "points/s",
+        ns = len(sizes)
+        gbs = ns * pts * 16 / (best_ms / 1e3) / 1e9
+        line.update({"metric": "four-step FFT, sizes 2^%d..2^%d, 2^25 points each: points/s (fastest split)" % (sizes[0], sizes[-1]),
+                     "value": ns * pts * world / (best_ms / 1e3), "unit": "points/s",
                      "ms_per_step": best_ms,
-                     "default_split_points_per_s": 6 * pts * world / (default_ms / 1e3),
+                     "default_split_points_per_s": ns * pts * world / (default_ms / 1e3),
                      "splits": table,
                      "config": {"workload": "one forward launch of 2^25 complex64 N(0,1) points per size, "
                                             "every admissible split n1 (64..1024, n/n1 in 128..1024)",
@@ -641,7 +647,7 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
                      "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
                                   "frac": gbs / peak, "peak_source": peak_src,
                                   "note": "16 B per point algorithmic; the intermediate adds 16 B"},
-                     "gpu_launches": 12 * args.steps, "clocks": clk})
+                     "gpu_launches": launches, "clocks": clk})
     elif args.workload in ("stft", "psd"):
         if args.workload == "stft":
             n, fft, hop = 1 << 24, 1024, 512
