@@ -16,8 +16,10 @@ FP64 FFT of sampled lines is <= 3e-6.
   c2c4096x256  N=4096 x 256 lines U[-1,1), forward then inverse per step, over a
                rotating pool of buffer sets larger than L2
   mixed        sizes 64..16384 plus 2^20, seeded counts U{1..512} up to 2^26
-               points, one CUDA graph per step (item-list column pass, TMA
-               column pass of the 2^20 class, item-list row pass, TMA row pass)
+               points, one CUDA graph per step: ONE launch of the persistent
+               queue kernel, which draws every 4096-point work item (four-step
+               columns, whole lines, four-step rows) from a device-side
+               descriptor array by atomic ticket
   conv         overlap-add convolution of 2^24 samples with 4095 taps
                (fftSize 8192): forward, then dx and dh, per step
   fconv        FusedConvolver (fftSize 4096) of 2^24 U[-1,1) samples with 512
@@ -560,11 +562,12 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
                      "gflop_note": "5 N log2 N per transform, summed over the classes",
                      "config": {"workload": "sizes 2^6..2^14 + 2^20, counts U{1..512} seeded, <= 2^26 points",
                                 "classes": classes, "points": mb.points,
-                                "graph": "one CUDA graph per step: four launches of the item kernel"},
+                                "graph": "one CUDA graph per step: a memset of the queue counters and ONE launch of "
+                                         "the queue kernel (k_fsq_queue) that draws every work item by atomic ticket"},
                      "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
                                   "frac": gbs / peak, "peak_source": peak_src,
                                   "note": "16 B per point algorithmic; four-step lines move 32 B"},
-                     "gpu_launches": 4 * args.steps, "clocks": clk})
+                     "gpu_launches": args.steps, "clocks": clk})
     elif args.workload == "c2c4096sweep":
         # config 1's step (one CUDA graph: forward, then inverse) over a range
         # of batches; a least-squares line through the per-launch times splits
