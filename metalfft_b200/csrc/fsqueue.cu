@@ -558,8 +558,8 @@ __device__ __forceinline__ bool q_wait_cols(const FsqQueueArgs& q, const QDesc& 
     return true;
 }
 
-__device__ __forceinline__ void red_release_add(int* p, int v) {
-    asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void red_relaxed_add(int* p, int v) {
+    asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ void bulk_wait_all_but_one() { asm volatile("cp.async.bulk.wait_group 1;" ::: "memory"); }
 
@@ -571,24 +571,50 @@ struct QDone {
     bool tma;
 };
 
-// thread 0: count finished COLS item d; `newer` = a bulk group committed after
-// d's own may still be pending.  The count is a release: d's tile stores
-// (made by every thread before a CTA barrier thread 0 has passed, or by its
-// bulk store, waited for here) are visible GPU-wide before ROWS items acquire
-// the count.
-__device__ __forceinline__ void q_count(const FsqQueueArgs& q, const QDone& d, bool newer) {
+// Finished COLS items thread 0 has not counted yet: their transforms x[0..n),
+// tma = one of them committed a bulk store.  A GPU-scope release costs thread 0
+// an L2 round trip (~2000 clocks, measured) while the CTA waits for it at the
+// next barrier, so up to Q_BATCH items share one.
+constexpr int Q_BATCH = 4;
+constexpr int Q_HOLD = Q_BATCH + 2;  // the loop counts at Q_BATCH; a wait or the end adds up to two first
+// in shared memory, used by thread 0 only (no registers held across the loop)
+struct QPend {
+    int x[Q_HOLD];
+    int n;
+    int tma;
+};
+
+// thread 0: remember finished item d (a COLS item) for the next count
+__device__ __forceinline__ void q_hold(QPend& p, const QDone& d) {
     if (d.x < 0) return;
-    if (d.tma) {
+    p.x[p.n++] = d.x;
+    p.tma |= d.tma ? 1 : 0;
+}
+
+// thread 0: count the held COLS items; `newer` = a bulk group committed after
+// theirs may still be pending.  One release for all of them (an acq_rel fence,
+// then relaxed reductions): their tile stores (made by every thread before a
+// CTA barrier thread 0 has passed, or by bulk stores, waited for here) are
+// visible GPU-wide before ROWS items acquire the counts.
+__device__ __forceinline__ void q_count(const FsqQueueArgs& q, QPend& p, bool newer) {
+    if (p.n == 0) return;
+    if (p.tma) {
         if (newer) bulk_wait_all_but_one();
         else bulk_wait_all();
         fence_proxy_async_global();
     }
-    red_release_add(q.counters + 1 + d.x, 1);
+    fence_acq_rel_gpu();
+#pragma unroll
+    for (int k = 0; k < p.n; ++k) red_relaxed_add(q.counters + 1 + p.x[k], 1);
+    p.n = 0;
+    p.tma = 0;
 }
 
 // Tickets are drawn one item ahead (the atomic's latency hides behind an
-// item's work), and a finished COLS item is counted two items later, when its
-// stores have long landed, so no thread stalls on either in steady state.
+// item's work), and a finished COLS item is counted at least two items later,
+// when its stores have long landed, so no thread stalls on either in steady
+// state; up to Q_BATCH of them are counted together, and everything held is
+// counted as soon as a CTA finishes an item that is not a COLS item.
 // A CTA counts everything it holds before it waits for a ROWS item's
 // columns, so no wait depends on its own work.
 template <bool INV>
@@ -599,6 +625,7 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
     __shared__ QDesc sh_desc[2];  // the item of each stage
     __shared__ QDesc sh_pre[2];   // descriptors prefetched for the next ticket
     __shared__ int sh_next, sh_ready;
+    __shared__ QPend held;  // thread 0: finished COLS items not counted yet
     float2* smem = reinterpret_cast<float2*>(fsq_raw + ((1024u - (smem_u32(fsq_raw) & 1023u)) & 1023u));
     const int n = q.a.nitems;
     const uint64_t pol = policy_evict_first();
@@ -616,6 +643,8 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
     int r1 = 1;     // thread 0: t1's column count was complete when read (or t1 is not a ROWS item)
     int pslot = 0;  // thread 0: sh_pre slot holding t1's descriptor (t2's is the other one)
     if (threadIdx.x == 0) {
+        held.n = 0;
+        held.tma = 0;
         mbar_init(&bar[0], FSQ_THREADS);
         mbar_init(&bar[1], FSQ_THREADS);
         fence_proxy_async_smem();
@@ -651,7 +680,8 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
     bool failed = false;
     for (;;) {
         if (threadIdx.x == 0) {
-            q_count(q, d2, d1.tma);
+            q_hold(held, d2);
+            if (held.n >= Q_BATCH || (held.n > 0 && d1.x < 0)) q_count(q, held, d1.tma);
             d2 = d1;
             d1 = QDone{-1, false};
             cp_async_wait<1>();  // t2's descriptor (all but the latest group, the data copies)
@@ -713,8 +743,9 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
             __syncthreads();  // every thread's tile stores precede the counts
             bool ok = true;
             if (threadIdx.x == 0) {
-                q_count(q, d2, d1.tma);
-                q_count(q, d1, false);
+                q_hold(held, d2);
+                q_hold(held, d1);
+                q_count(q, held, false);
                 d1 = d2 = QDone{-1, false};
                 ok = q_wait_cols(q, sh_desc[s ^ 1]);
             }
@@ -737,8 +768,9 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
             mbar_wait(&bar[0], ph[0]);
             mbar_wait(&bar[1], ph[1]);
         } else {
-            q_count(q, d2, d1.tma);
-            q_count(q, d1, false);
+            q_hold(held, d2);
+            q_hold(held, d1);
+            q_count(q, held, false);
         }
         bulk_wait_all();
     }
