@@ -622,8 +622,11 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
     k_fsq_queue(const __grid_constant__ FsqQueueArgs q, int* dev_err) {
     extern __shared__ __align__(1024) unsigned char fsq_raw[];
     __shared__ __align__(8) uint64_t bar[2];
-    __shared__ QDesc sh_desc[2];  // the item of each stage
-    __shared__ QDesc sh_pre[2];   // descriptors prefetched for the next ticket
+    // descriptor ring: the item of iteration j in slot j % 4 from the time it is
+    // drawn (two tickets ahead) until it is done, so that no descriptor is
+    // copied (a shared-memory access of thread 0 costs hundreds of clocks while
+    // the rest of the CTA waits for it at the next barrier)
+    __shared__ QDesc sh_q[4];
     __shared__ int sh_next, sh_ready;
     __shared__ QPend held;  // thread 0: finished COLS items not counted yet
     float2* smem = reinterpret_cast<float2*>(fsq_raw + ((1024u - (smem_u32(fsq_raw) & 1023u)) & 1023u));
@@ -640,8 +643,9 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
     // early read fell short.
     bool first_ok = true;
     int t1 = n, t2 = n, t3 = n;
-    int r1 = 1;     // thread 0: t1's column count was complete when read (or t1 is not a ROWS item)
-    int pslot = 0;  // thread 0: sh_pre slot holding t1's descriptor (t2's is the other one)
+    // thread 0, t1's readiness as read early: 2 = not a ROWS item, 1 = a ROWS item
+    // whose column count was complete, 0 = one whose count fell short
+    int r1 = 2;
     if (threadIdx.x == 0) {
         held.n = 0;
         held.tma = 0;
@@ -657,59 +661,55 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
                 t2 = atomicAdd(q.counters, 1);
                 if (t2 < n) t3 = atomicAdd(q.counters, 1);
                 const QDesc d1v = q.a.items[t1];
-                sh_pre[0] = d1v;
-                r1 = d1v.kind != FSQ_ROWS || ld_relaxed_gpu(q.counters + 1 + d1v.xform) >= q_cols_needed(d1v.logn);
+                sh_q[1] = d1v;
+                r1 = d1v.kind != FSQ_ROWS ? 2 : ld_relaxed_gpu(q.counters + 1 + d1v.xform) >= q_cols_needed(d1v.logn);
             }
-            sh_desc[0] = dc;
+            sh_q[0] = dc;
             first_ok = q_wait_cols(q, dc);
         }
-        if (t2 < n) q_prefetch_desc(q, t2, &sh_pre[1]);
+        if (t2 < n) q_prefetch_desc(q, t2, &sh_q[2]);
         else cp_async_commit();
     }
     if (__syncthreads_or(!first_ok)) {
         if (threadIdx.x == 0) report_device_error(dev_err, DEV_ERR_QUEUE_TIMEOUT);
         return;
     }
-    int cur = sh_next;
-    if (cur >= n) return;
-    q_issue(q, sh_desc[0], smem, &bar[0], pol);
+    if (sh_next >= n) return;
+    q_issue(q, sh_q[0], smem, &bar[0], pol);
     if (threadIdx.x == 0) cp_async_commit();  // thread 0's groups: descriptor, data, descriptor, ...
     uint32_t ph[2] = {0u, 0u};
-    int s = 0;
     QDone d1{-1, false}, d2{-1, false};  // thread 0: the previous item, the one before it
     bool failed = false;
-    for (;;) {
+    for (int j = 0;; ++j) {  // iteration j computes the item of slot j % 4 in stage s = j % 2
+        const int s = j & 1;
         if (threadIdx.x == 0) {
             q_hold(held, d2);
             if (held.n >= Q_BATCH || (held.n > 0 && d1.x < 0)) q_count(q, held, d1.tma);
             d2 = d1;
             d1 = QDone{-1, false};
             cp_async_wait<1>();  // t2's descriptor (all but the latest group, the data copies)
-            const int nx = t1;
+            const int nx = t1;   // the item of iteration j + 1
             int ready = 1;
-            if (nx < n) {
-                const QDesc& dx = sh_pre[pslot];
-                if (dx.kind == FSQ_ROWS) {
-                    ready = r1 || ld_acquire_gpu(q.counters + 1 + dx.xform) >= q_cols_needed(dx.logn);
-                    if (ready) fence_acq_rel_gpu();  // its columns' stores before this CTA's reads
-                }
-                sh_desc[s ^ 1] = dx;
+            if (nx < n && !r1) {
+                const QDesc& dx = sh_q[(j + 1) & 3];  // a ROWS item whose count fell short when read early
+                ready = ld_acquire_gpu(q.counters + 1 + dx.xform) >= q_cols_needed(dx.logn);
             }
+            // a ROWS item: its columns' stores before this CTA's reads
+            if (nx < n && ready && r1 != 2) fence_acq_rel_gpu();
             // shift the look-ahead: t2 -> t1 (read its count now), t3 -> t2 (prefetch its descriptor)
             t1 = t2;
-            r1 = 1;
+            r1 = 2;  // 2: not a ROWS item
             if (t1 < n) {
-                const QDesc& dn = sh_pre[pslot ^ 1];
+                const QDesc& dn = sh_q[(j + 2) & 3];
                 if (dn.kind == FSQ_ROWS) r1 = ld_relaxed_gpu(q.counters + 1 + dn.xform) >= q_cols_needed(dn.logn);
             }
             t2 = t3;
             if (t2 < n) {
                 t3 = atomicAdd(q.counters, 1);
-                q_prefetch_desc(q, t2, &sh_pre[pslot]);
+                q_prefetch_desc(q, t2, &sh_q[(j + 3) & 3]);  // the slot of iteration j - 1, done
             } else {
                 cp_async_commit();
             }
-            pslot ^= 1;
             bulk_wait_read_all();  // the other stage is no longer read by a bulk store
             sh_next = nx;
             sh_ready = ready;
@@ -717,7 +717,7 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
         __syncthreads();
         const int nx = sh_next;
         const bool ready = sh_ready != 0;
-        if (nx < n && ready) q_issue(q, sh_desc[s ^ 1], smem + (s ^ 1) * QSTAGE, &bar[s ^ 1], pol);
+        if (nx < n && ready) q_issue(q, sh_q[(j + 1) & 3], smem + (s ^ 1) * QSTAGE, &bar[s ^ 1], pol);
         if (threadIdx.x == 0 && (ready || nx >= n)) cp_async_commit();
         const bool landed = mbar_wait(&bar[s], ph[s]);
         ph[s] ^= 1u;
@@ -725,7 +725,7 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
             failed = true;
             break;
         }
-        const QDesc& dc = sh_desc[s];
+        const QDesc& dc = sh_q[j & 3];
         const Work w = q_work(dc);
         float2* st = smem + s * QSTAGE;
         if (dc.grp >= 0) {
@@ -747,19 +747,17 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
                 q_hold(held, d1);
                 q_count(q, held, false);
                 d1 = d2 = QDone{-1, false};
-                ok = q_wait_cols(q, sh_desc[s ^ 1]);
+                ok = q_wait_cols(q, sh_q[(j + 1) & 3]);
             }
             if (__syncthreads_or(!ok)) {
                 failed = true;
                 break;
             }
-            q_issue(q, sh_desc[s ^ 1], smem + (s ^ 1) * QSTAGE, &bar[s ^ 1], pol);
+            q_issue(q, sh_q[(j + 1) & 3], smem + (s ^ 1) * QSTAGE, &bar[s ^ 1], pol);
             if (threadIdx.x == 0) cp_async_commit();
         }
         __syncthreads();  // every read of stage s (and of its descriptor) is done before either is refilled
         if (nx >= n) break;
-        cur = nx;
-        s ^= 1;
     }
     if (threadIdx.x == 0) {
         if (failed) {
