@@ -295,7 +295,6 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
     // the azimuth transform and, for the gradient, the transform of conj(G)
     // through one call site (two inlined transforms get interleaved and need
     // more registers)
-    double lsum = 0.0;
 #pragma unroll 1
     for (int ph = 0; ph < (GRAD ? 2 : 1); ++ph) {
         fft_regs<NA, SAR_E, false>(v, t, ColLine<C>{smem, c}, tw);  // ph 0: v[m] = I[k = t + m*T][col]
@@ -327,37 +326,35 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
             if (t == 0) image_scale[col] = s;
         }
         if constexpr (GRAD) {
+            double lsum = 0.0;
 #pragma unroll
             for (int m = 0; m < SAR_E; ++m) {
                 const float a2 = v[m].x * v[m].x + v[m].y * v[m].y;
                 lsum += (double)a2 * (double)a2;
                 v[m] = make_float2(4.f * a2 * v[m].x, -4.f * a2 * v[m].y);  // conj(G)
             }
+            // the warp's part of the loss waits in shared memory, not in registers,
+            // while conj(G) is transformed
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+            if ((threadIdx.x & 31) == 0) lred[threadIdx.x >> 5] = lsum;
         }
     }
     if constexpr (GRAD) {
-        float d[SAR_E];
+        // per pulse p = t + m*T: -Im(u conj(B)) with v = conj(B), i.e. -Im(u v),
+        // summed over the C columns of the tile (c is the low part of the lane id)
+        // and stored as soon as it is formed
 #pragma unroll
         for (int m = 0; m < SAR_E; ++m) {
             const int p = t + m * T;
             const float2 u0 = ld_rc(rcol + m * rstep);
             const float s = __ldg(rc_scale + p);
             const float2 u = make_float2(u0.x * s, u0.y * s);
-            // -Im(u conj(B)) with v = conj(B): -Im(u v)
-            d[m] = -(u.x * v[m].y + u.y * v[m].x);
+            float d = -(u.x * v[m].y + u.y * v[m].x);
+#pragma unroll
+            for (int o = 1; o < C && o < 32; o <<= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+            if (c == 0) dphi_part[tile * NA + p] = d;
         }
-        // sum over the C columns of the tile: c is the low part of the lane id
-#pragma unroll
-        for (int m = 0; m < SAR_E; ++m)
-#pragma unroll
-            for (int o = 1; o < C && o < 32; o <<= 1) d[m] += __shfl_xor_sync(0xffffffffu, d[m], o);
-        if (c == 0) {
-#pragma unroll
-            for (int m = 0; m < SAR_E; ++m) dphi_part[tile * NA + t + m * T] = d[m];
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-        if ((threadIdx.x & 31) == 0) lred[threadIdx.x >> 5] = lsum;
         __syncthreads();
         if (threadIdx.x == 0) {
             double tot = 0.0;
