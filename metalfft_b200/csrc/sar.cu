@@ -210,9 +210,13 @@ __device__ __forceinline__ float2 ld_rc(const __half2* p) { return __half22float
 __device__ __forceinline__ float2 ld_rc(const float2* p) { return *p; }
 
 // pass A: range compression of one pulse per CTA; RC = __half2 (FP16 with a
-// per-pulse scale) or float2 (FP32, scale 1)
+// per-pulse scale) or float2 (FP32, scale 1).  Up to NR = 8192 two CTAs share
+// an SM (64 registers a thread at 512 threads, without spills; 2 x 70 KB of
+// shared memory): twice the warps to hide the exchanges' latency.
+template <int NR>
+constexpr int range_min_blocks() { return NR <= 8192 ? 2 : 1; }
 template <int NR, class RC>
-__global__ void __launch_bounds__(NR / SAR_E) k_sar_range(const __half2* __restrict__ raw, const float* __restrict__ pscale,
+__global__ void __launch_bounds__(NR / SAR_E, range_min_blocks<NR>()) k_sar_range(const __half2* __restrict__ raw, const float* __restrict__ pscale,
                                                            const float* __restrict__ phase, const float2* __restrict__ H,
                                                            const float2* __restrict__ tw, RC* __restrict__ rc,
                                                            float* __restrict__ rc_scale) {
@@ -533,6 +537,13 @@ cudaError_t prep_range() {
     cudaError_t e = cudaFuncSetAttribute(k_sar_range<NR, __half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_sar_range<NR, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    // the largest shared-memory carveout, so that range_min_blocks CTAs fit on an SM
+    e = cudaFuncSetAttribute(k_sar_range<NR, __half2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_sar_range<NR, float2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_sar_rcmc<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, NR * 8);
 }
