@@ -545,7 +545,10 @@ cudaError_t prep_range() {
     e = cudaFuncSetAttribute(k_sar_range<NR, float2>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_sar_rcmc<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, NR * 8);
+    e = cudaFuncSetAttribute(k_sar_rcmc<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, NR * 8);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_sar_rcmc<NR>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                cudaSharedmemCarveoutMaxShared);
 }
 template <int NA, bool IMAGE, bool GRAD, bool INV, class RC>
 cudaError_t prep_az1() {
