@@ -258,7 +258,11 @@ MFFT_API int mfft_fourstep_noalloc(const void* in, void* out, int64_t n, int64_t
  * mixed sizes; it generalises forward(batch:) (MetalFFT.swift:108-133).
  * Sizes up to 4096 run as whole lines, larger ones as four-step transforms
  * (a column pass into an intermediate buffer of the handle holding every
- * four-step point, then a row pass). */
+ * four-step point, then a row pass).  One mfft_multi_exec is one kernel
+ * launch: persistent CTAs draw 4096-point work items (column items, whole
+ * lines, row items) from a device-side descriptor array by atomic ticket, and
+ * a row item starts once its transform's column items are counted done (a
+ * bounded wait; MFFT_ERR_TIMEOUT when it gives up). */
 typedef struct mfft_multi_desc {
     int64_t n;
     int64_t count;
