@@ -455,14 +455,16 @@ def run_reference(args, rank, world):
     from oracle import oracle as O
     B = args.batch
     x = make_input(B, 0)
+    # every host core this process may run on: under torchrun OMP_NUM_THREADS is
+    # 1, but the other ranks exit without work
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     for _ in range(args.warmup):
-        O.ref_fft(x)
+        O.ref_fft(x, threads=cores)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.ref_fft(x)
+        O.ref_fft(x, threads=cores)
     dt = time.perf_counter() - t0
     v = args.steps * B / dt
-    cores = O.max_threads()
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "transforms/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
