@@ -64,3 +64,27 @@ def test_two_gloo_ranks():
     got = np.concatenate([r[3] for r in res])
     assert np.array_equal(got, full)
     assert all(r[4] == 3.0 for r in res)  # max over ranks of 1.5 and 3.0
+
+
+def test_reference_arm_under_torchrun_two_ranks():
+    """`bench.py --impl reference` launched as the driver launches every arm
+    for N > 1: rank 0 alone times the host path and prints one JSON line, on
+    every core the process may use although torchrun sets OMP_NUM_THREADS=1;
+    the other rank exits 0 without work."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
+           os.path.join(root, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1",
+           "--batch", "64"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, out.stdout
+    d = lines[0]
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    assert d["cpu_baseline"]["cores"] == cores
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
