@@ -37,6 +37,8 @@ FP64 FFT of sampled lines is <= 3e-6.
                every frame's complex spectrum and |X|^2, one launch per step
   psd          Welch PSD of 2^26 N(0,1) samples, fftSize 4096, hop 2048,
                Hann, one launch (+ a fixed-order reduction) per step
+  r2c          real-input FFT, N=4096: R2C of 2^15 real N(0,1) lines (2049 bins
+               each), then C2R of those bins back, per step
   xspec        cross-spectral density matrix of 8 channels x 2^23 samples
                (a shared N(0,1) component plus N(0,1) noise per channel),
                fftSize 1024, hop 512, Hann: powers, 28 cross-spectra and the
@@ -81,7 +83,7 @@ def parse():
     p.add_argument("--fs-log2", default="15-20",
                    help="fourstep workload: log2 sizes to sweep, a range lo-hi or one value")
     p.add_argument("--workload", default="tc4096", choices=["tc4096", "c2c4096x256", "mixed", "conv", "fconv", "sar", "sarfocus", "stft",
-                                                        "psd", "xspec", "fourstep", "c2c4096sweep"])
+                                                        "psd", "xspec", "fourstep", "c2c4096sweep", "r2c"])
     return p.parse_args()
 
 
@@ -418,6 +420,17 @@ def cpu_baseline_other(workload, seconds=8.0):
         fn = (lambda: O.stft64(x, fft, hop, w)) if workload == "stft" else (lambda: O.welch64(x, fft, hop, w, 48000.0))
         units, unit = n, "samples/s"
         what = "2^20 samples, fftSize %d, hop %d, Hann: FP64 per-frame restatement" % (fft, hop)
+    elif workload == "r2c":
+        # the reference's real-input path: the samples packed as complex with a
+        # zero imaginary part (Convolve.swift:47-53, FFTAnalyzer.swift:98-100),
+        # a complex forward transform, and a complex inverse of the bins back
+        x = (rng.standard_normal((256, 4096)).astype(np.float32) + 0j).astype(np.complex64)
+
+        def fn():
+            O.ref_fft(O.ref_fft(x), inverse=True)
+        units, unit = 512, "transforms/s"
+        what = "256 real lines of N=4096 packed as complex (zero imaginary), forward then inverse, FP32 radix-4 " \
+               "Stockham restatement"
     elif workload == "xspec":
         n = 1 << 17
         x = rng.standard_normal((8, n))
@@ -737,6 +750,42 @@ def run_other(args, M, rank, world, dist, barrier, uuid):
                                   "frac": gbs / peak, "peak_source": peak_src,
                                   "note": "x read and y written once; the FFT arithmetic bounds it"},
                      "gpu_launches": args.steps, "clocks": clk})
+    elif args.workload == "r2c":
+        n, lines = 4096, 1 << 15
+        h = n // 2 + 1
+        rng = np.random.default_rng(SEED + rank)
+        x = torch.from_numpy(rng.standard_normal((lines, n), dtype=np.float32)).cuda()
+        X = torch.empty((lines, h), dtype=torch.complex64, device="cuda")
+        y = torch.empty_like(x)
+        f = M.MetalFFT(n)
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        P = lambda a: ctypes.c_void_p(a.data_ptr())  # noqa: E731
+
+        def step(i):
+            M._check(M.lib.mfft_exec_r2c(f._plan, P(x), P(X), lines, M.DEVICE, st))
+            M._check(M.lib.mfft_exec_c2r(f._plan, P(X), P(y), lines, M.DEVICE, st))
+        ms_max, ms, clk = timed(step, args.steps, args.warmup, barrier, dist, uuid)
+        assert M.lib.mfft_context_check(M.shared_context()) == 0
+        # bins of sampled lines against an FP64 rfft, and the round trip
+        rows = np.linspace(0, lines - 1, 16).astype(np.int64)
+        xs = x[rows].double().cpu().numpy()
+        Xs = X[rows].cpu().numpy().astype(np.complex128)
+        ref = np.fft.rfft(xs, axis=1)
+        err = float(np.linalg.norm(Xs - ref) / np.linalg.norm(ref))
+        err_rt = float(torch.linalg.vector_norm(y - x) / torch.linalg.vector_norm(x))
+        per_line = 4 * n + 8 * h  # real samples one way, bins the other
+        algo = 2 * lines * per_line
+        gbs = algo / (ms / args.steps / 1e3) / 1e9
+        line.update({"metric": "real-input FFT N=4096: transforms/s (R2C forward + C2R inverse, each counted)",
+                     "value": 2 * lines * world * args.steps / (ms_max / 1e3), "unit": "transforms/s",
+                     "ms_per_step": ms_max / args.steps, "rel_rms": err, "round_trip_rel": err_rt,
+                     "config": {"workload": "2^15 real lines of N=4096, N(0,1) seeded: R2C (2049 bins per line), "
+                                            "then C2R of the bins back",
+                                "l2": "512 MiB of real samples and 537 MB of bins per direction > L2"},
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                  "frac": gbs / peak, "peak_source": peak_src,
+                                  "note": "4 B per real sample + 8 B per bin, each way"},
+                     "gpu_launches": 2 * args.steps, "clocks": clk})
     elif args.workload == "xspec":
         C, n, fft, hop = 8, 1 << 23, 1024, 512
         rng = np.random.default_rng(SEED + rank)
