@@ -575,7 +575,7 @@ struct QDone {
 // tma = one of them committed a bulk store.  A GPU-scope release costs thread 0
 // an L2 round trip (~2000 clocks, measured) while the CTA waits for it at the
 // next barrier, so up to Q_BATCH items share one.
-constexpr int Q_BATCH = 4;
+constexpr int Q_BATCH = 8;
 constexpr int Q_HOLD = Q_BATCH + 2;  // the loop counts at Q_BATCH; a wait or the end adds up to two first
 // in shared memory, used by thread 0 only (no registers held across the loop)
 struct QPend {
