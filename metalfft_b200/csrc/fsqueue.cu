@@ -452,11 +452,6 @@ __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
     return v;
 }
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
-__device__ __forceinline__ int ld_relaxed_gpu(const int* p) {
-    int v;
-    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 // An item with its transform's offsets, read from the queue one ticket ahead
@@ -637,15 +632,12 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
     // Thread 0 works three tickets ahead of the item it issues: t1 (its
     // descriptor in shared memory, its readiness read one iteration ago), t2
     // (descriptor landed this iteration, readiness read now), t3 (the atomic
-    // draw, consumed next iteration).  A ROWS item's column count is read
-    // relaxed one iteration early; a ROWS item is issued after an acquire fence
-    // once that count is complete, and re-read (and waited for) only when the
-    // early read fell short.
+    // draw, consumed next iteration).  A ROWS item is issued once an acquire
+    // load of its transform's column count finds it complete (one load, no
+    // fence), and waited for only when that load falls short.
     bool first_ok = true;
     int t1 = n, t2 = n, t3 = n;
-    // thread 0, t1's readiness as read early: 2 = not a ROWS item, 1 = a ROWS item
-    // whose column count was complete, 0 = one whose count fell short
-    int r1 = 2;
+    bool rows1 = false;  // thread 0: t1 is a ROWS item
     if (threadIdx.x == 0) {
         held.n = 0;
         held.tma = 0;
@@ -662,7 +654,7 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
                 if (t2 < n) t3 = atomicAdd(q.counters, 1);
                 const QDesc d1v = q.a.items[t1];
                 sh_q[1] = d1v;
-                r1 = d1v.kind != FSQ_ROWS ? 2 : ld_relaxed_gpu(q.counters + 1 + d1v.xform) >= q_cols_needed(d1v.logn);
+                rows1 = d1v.kind == FSQ_ROWS;
             }
             sh_q[0] = dc;
             first_ok = q_wait_cols(q, dc);
@@ -690,18 +682,17 @@ __global__ void __launch_bounds__(FSQ_THREADS, FSQ_CTAS_PER_SM)
             cp_async_wait<1>();  // t2's descriptor (all but the latest group, the data copies)
             const int nx = t1;   // the item of iteration j + 1
             int ready = 1;
-            if (nx < n && !r1) {
-                const QDesc& dx = sh_q[(j + 1) & 3];  // a ROWS item whose count fell short when read early
+            if (nx < n && rows1) {
+                // the acquire orders its columns' stores before this CTA's reads
+                const QDesc& dx = sh_q[(j + 1) & 3];
                 ready = ld_acquire_gpu(q.counters + 1 + dx.xform) >= q_cols_needed(dx.logn);
             }
-            // a ROWS item: its columns' stores before this CTA's reads
-            if (nx < n && ready && r1 != 2) fence_acq_rel_gpu();
-            // shift the look-ahead: t2 -> t1 (read its count now), t3 -> t2 (prefetch its descriptor)
+            // shift the look-ahead: t2 -> t1, t3 -> t2 (prefetch its descriptor)
             t1 = t2;
-            r1 = 2;  // 2: not a ROWS item
+            rows1 = false;
             if (t1 < n) {
                 const QDesc& dn = sh_q[(j + 2) & 3];
-                if (dn.kind == FSQ_ROWS) r1 = ld_relaxed_gpu(q.counters + 1 + dn.xform) >= q_cols_needed(dn.logn);
+                rows1 = dn.kind == FSQ_ROWS;
             }
             t2 = t3;
             if (t2 < n) {
