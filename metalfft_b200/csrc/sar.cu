@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
     // more registers)
 #pragma unroll 1
     for (int ph = 0; ph < (GRAD ? 2 : 1); ++ph) {
-        fft_regs<NA, SAR_E, false>(v, t, ColLine<C>{smem, c}, tw);  // ph 0: v[m] = I[k = t + m*T][col]
+        fft_regs<NA, SAR_E, false>(v, t, ColXorLine<C>{smem, c}, tw);  // ph 0: v[m] = I[k = t + m*T][col]
         if (ph == 1) break;                                          // ph 1: v[m] = conj(B[p]), p = t + m*T
         if constexpr (INV) {
             // inverse transform along azimuth: conj(FFT(conj(x))) / NA

@@ -42,6 +42,19 @@ struct ColLine {
     int c;
     __device__ __forceinline__ float2& operator[](int i) const { return base[i * C + c]; }
 };
+// C lines interleaved element by element, the element index's low three bits
+// XORed with its bits 4-6: line c, element i at (i ^ ((i >> 4) & 7))*C + c.
+// With C = 2 or 4 and radix-16 passes, the first pass's writes (elements
+// 16j + r, j = the thread) land 16*C float2 apart, all on one bank, in
+// ColLine; the XOR moves consecutive threads to different 8-byte slots, while
+// the reads (consecutive i) and the later passes' writes (consecutive i within
+// a 16-element group) stay conflict-free.
+template <int C>
+struct ColXorLine {
+    float2* base;
+    int c;
+    __device__ __forceinline__ float2& operator[](int i) const { return base[(i ^ ((i >> 4) & 7)) * C + c]; }
+};
 // C lines interleaved with an XOR swizzle, so that both a warp walking one
 // line (i consecutive, c fixed) and a warp walking across lines (c
 // consecutive, i fixed) hit distinct banks: line c, element i at
