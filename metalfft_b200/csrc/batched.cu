@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
     const int t = threadIdx.x % T;
     const long long f = (long long)blockIdx.x * FPB + lf;
     const bool ok = f < batch;
-    const PadLine buf{smem + lf * spad_size(N)};
+    const PadLineS buf{smem + lf * spad_size(N)};
     float2 v[E];
     grid_dep_wait();
     if (ok) {
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(SPlan<N, E>::T * FPB)
             }
             return;
         }
-        fft_regs<N, E, WS>(v, t, PadLine{buf + lf * spad_size(N)}, tw);
+        fft_regs<N, E, WS>(v, t, PadLineS{buf + lf * spad_size(N)}, tw);
         fence_proxy_async_smem();  // order this thread's exchange writes before the next bulk copy
         __syncthreads();           // every exchange access of this buffer is done
         if (threadIdx.x == 0) {

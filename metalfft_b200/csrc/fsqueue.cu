@@ -120,7 +120,7 @@ __device__ __forceinline__ void do_lines(float2* st, float2* __restrict__ out, l
         if constexpr (INV) v[m].y = -v[m].y;
     }
     __syncthreads();  // the raw item is in registers; the stage becomes the exchange area
-    fft_regs<L, 16, (T <= 32)>(v, t, PadLine{st + u * spad_size(L)}, tw);
+    fft_regs<L, 16, (T <= 32)>(v, t, PadLineS{st + u * spad_size(L)}, tw);
     if (u < lines) {
         float2* dst = out + off + (long long)u * L + t;
 #pragma unroll
@@ -146,7 +146,7 @@ __device__ __forceinline__ void do_cols(float2* st, float2* __restrict__ mid, in
         if constexpr (INV) v[m].y = -v[m].y;
     }
     __syncthreads();
-    fft_regs<L, 16, (T <= 32)>(v, t, PadLine{st + c * spad_size(L)}, tw);
+    fft_regs<L, 16, (T <= 32)>(v, t, PadLineS{st + c * spad_size(L)}, tw);
     // W_n^{col*k1}, k1 = t + m*T: base W^{col*t} times W^{col*T*m}, the latter
     // a product of at most four of W^{col*T*{1,2,4,8}} (warp-uniform loads);
     // every exponent stays below n
@@ -190,7 +190,7 @@ __device__ __forceinline__ void do_rows(float2* st, const float2* mid_rows, floa
     // write-back (32 KiB = 256 lines of 128 bytes, one per thread)
     discard_l2_line(reinterpret_cast<const char*>(mid_rows) + 128 * threadIdx.x);
     __syncthreads();
-    fft_regs<L, 16, (T <= 32)>(v, t, PadLine{st + r * spad_size(L)}, tw);
+    fft_regs<L, 16, (T <= 32)>(v, t, PadLineS{st + r * spad_size(L)}, tw);
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < 16; ++m)

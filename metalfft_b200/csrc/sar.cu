@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(NR / SAR_E, range_min_blocks<NR>()) k_sar_rang
     // (two inlined transforms get interleaved and need more registers)
 #pragma unroll 1
     for (int ph = 0; ph < 2; ++ph) {
-        fft_regs<NR, SAR_E, (T <= 32)>(v, t, PadLine{smem}, tw);
+        fft_regs<NR, SAR_E, (T <= 32)>(v, t, PadLineS{smem}, tw);
         if (ph == 0) {
 #pragma unroll
             for (int m = 0; m < SAR_E; ++m) v[m] = cconj(cmul(v[m], __ldg(H + t + m * T)));
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(AzGeom<NA>::THREADS)
     // more registers)
 #pragma unroll 1
     for (int ph = 0; ph < (GRAD ? 2 : 1); ++ph) {
-        fft_regs<NA, SAR_E, false>(v, t, ColXorLine<C>{smem, c}, tw);  // ph 0: v[m] = I[k = t + m*T][col]
+        fft_regs<NA, SAR_E, false>(v, t, ColPadLine<C>{smem, c}, tw);  // ph 0: v[m] = I[k = t + m*T][col]
         if (ph == 1) break;                                          // ph 1: v[m] = conj(B[p]), p = t + m*T
         if constexpr (INV) {
             // inverse transform along azimuth: conj(FFT(conj(x))) / NA
@@ -528,7 +528,7 @@ void l_range(int grid, cudaStream_t s, const __half2* raw, const float* ps, cons
 template <int NA, bool IMAGE, bool GRAD, bool INV = false, class RC = __half2>
 void l_az(int grid, cudaStream_t s, const RC* rc, const float* rcs, long long nr, const float2* tw, __half2* img,
           float* imgs, float* dp, double* lp) {
-    k_sar_azimuth<NA, IMAGE, GRAD, INV, RC><<<grid, AzGeom<NA>::THREADS, NA * AzGeom<NA>::C * 8, s>>>(
+    k_sar_azimuth<NA, IMAGE, GRAD, INV, RC><<<grid, AzGeom<NA>::THREADS, spad_size(NA) * AzGeom<NA>::C * 8, s>>>(
         rc, rcs, nr, tw, img, imgs, dp, lp);
 }
 template <int NR>
@@ -553,7 +553,7 @@ cudaError_t prep_range() {
 template <int NA, bool IMAGE, bool GRAD, bool INV, class RC>
 cudaError_t prep_az1() {
     return cudaFuncSetAttribute(k_sar_azimuth<NA, IMAGE, GRAD, INV, RC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                NA * AzGeom<NA>::C * 8);
+                                spad_size(NA) * AzGeom<NA>::C * 8);
 }
 template <int NA>
 cudaError_t prep_az() {

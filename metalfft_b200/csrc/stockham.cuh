@@ -35,6 +35,28 @@ struct PadLine {
     float2* base;
     __device__ __forceinline__ float2& operator[](int i) const { return base[spad(i)]; }
 };
+// The same layout, declared splittable: kPadStride says the layout is
+// base + spad(i) * kPadStride, so the passes address it as
+// at(a)[spad(b) * kPadStride] wherever spad(a + b) = spad(a) + spad(b) (b a
+// multiple of 16, or a a multiple of 16 and b < 16): one address computation
+// per group of R writes and one per thread for the reads, the rest constant
+// offsets.  Kept apart from PadLine because the split is not a gain in every
+// kernel (the real-input FFT measured slower with it).
+struct PadLineS {
+    float2* base;
+    static constexpr int kPadStride = 1;
+    __device__ __forceinline__ float2& operator[](int i) const { return base[spad(i)]; }
+    __device__ __forceinline__ float2* at(int i) const { return base + spad(i); }
+};
+// kPadStride of a layout, 0 for layouts without one.
+template <class Buf>
+__host__ __device__ constexpr auto pad_stride_of(int) -> decltype(Buf::kPadStride) {
+    return Buf::kPadStride;
+}
+template <class Buf>
+__host__ __device__ constexpr int pad_stride_of(long) {
+    return 0;
+}
 // C lines interleaved element by element: line c, element i at i*C + c.
 template <int C>
 struct ColLine {
@@ -42,18 +64,20 @@ struct ColLine {
     int c;
     __device__ __forceinline__ float2& operator[](int i) const { return base[i * C + c]; }
 };
-// C lines interleaved element by element, the element index's low three bits
-// XORed with its bits 4-6: line c, element i at (i ^ ((i >> 4) & 7))*C + c.
-// With C = 2 or 4 and radix-16 passes, the first pass's writes (elements
-// 16j + r, j = the thread) land 16*C float2 apart, all on one bank, in
-// ColLine; the XOR moves consecutive threads to different 8-byte slots, while
-// the reads (consecutive i) and the later passes' writes (consecutive i within
-// a 16-element group) stay conflict-free.
+// C lines interleaved element by element over the padded index: line c,
+// element i at spad(i)*C + c (splittable, kPadStride = C).  With C = 2 or 4
+// and radix-16 passes, the first pass's writes (elements 16j + r, j = the
+// thread) land 16*C float2 apart, all on one bank, in ColLine; the pad puts
+// consecutive threads 17*C float2 apart, on different banks, while the reads
+// (consecutive i) and the later passes' writes (consecutive i within a
+// 16-element group) stay conflict-free.
 template <int C>
-struct ColXorLine {
+struct ColPadLine {
     float2* base;
     int c;
-    __device__ __forceinline__ float2& operator[](int i) const { return base[(i ^ ((i >> 4) & 7)) * C + c]; }
+    static constexpr int kPadStride = C;
+    __device__ __forceinline__ float2& operator[](int i) const { return base[spad(i) * C + c]; }
+    __device__ __forceinline__ float2* at(int i) const { return base + spad(i) * C + c; }
 };
 // C lines interleaved with an XOR swizzle, so that both a warp walking one
 // line (i consecutive, c fixed) and a warp walking across lines (c
@@ -76,6 +100,11 @@ struct StockhamPass {
         constexpr int NS = PL::span(P);
         constexpr int B = E / R;
         constexpr int T = PL::T;
+        // padded layouts: one address per group of R writes (and per thread for the
+        // reads), the rest constant offsets, where the split is exact
+        constexpr int S = pad_stride_of<Buf>(0);
+        constexpr bool WSPLIT = S > 0 && (NS % 16 == 0 || (NS == 1 && R == 16));
+        constexpr bool RSPLIT = S > 0 && T % 16 == 0;
         if constexpr (NS > 1) {
 #pragma unroll
             for (int b = 0; b < B; ++b) {
@@ -91,12 +120,24 @@ struct StockhamPass {
                 const int j = t + b * T;
                 const int k = j & (NS - 1);
                 const int d = (j - k) * R + k;
+                if constexpr (WSPLIT) {
+                    float2* p = buf.at(d);
 #pragma unroll
-                for (int r = 0; r < R; ++r) buf[d + r * NS] = v[b + r * B];
+                    for (int r = 0; r < R; ++r) p[spad(r * NS) * S] = v[b + r * B];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) buf[d + r * NS] = v[b + r * B];
+                }
             }
             line_sync<WS>();
+            if constexpr (RSPLIT) {
+                const float2* p = buf.at(t);
 #pragma unroll
-            for (int m = 0; m < E; ++m) v[m] = buf[t + m * T];
+                for (int m = 0; m < E; ++m) v[m] = p[spad(m * T) * S];
+            } else {
+#pragma unroll
+                for (int m = 0; m < E; ++m) v[m] = buf[t + m * T];
+            }
             line_sync<WS>();
             StockhamPass<N, E, P + 1, WS>::run(v, t, buf, tw);
         }
