@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(SpGeom<FFT>::THREADS, SpGeom<FFT>::MINB)
     constexpr bool ACC_SMEM = G::template acc_smem<PLANES>();
     extern __shared__ __align__(16) float2 smem[];
     const int lf = threadIdx.x / T, t = threadIdx.x % T;
-    const PadLine buf{smem + lf * spad_size(FFT)};
+    const PadLineS buf{smem + lf * spad_size(FFT)};
     const long long u = (long long)blockIdx.x * G::LINES + lf;
     float* acc = ACC_SMEM ? reinterpret_cast<float*>(smem + G::XCH) + lf * PLANES * FFT : part + u * PLANES * FFT;
 #pragma unroll
